@@ -1,0 +1,514 @@
+#!/usr/bin/env python
+"""Benchmark of the cone-beam FDK hot path on B200.
+
+Workload (one step): a cone-beam scan of 600 views (486 x 384 detector, 0.299 mm,
+SOD 440 / SDD 680 mm, 40 seeded random ellipsoids in a 60 mm sphere, raw uint16 counts
+with flat ~ 50000 +/- 2 %, dark ~ 100 +/- 5 and Poisson noise) is ingested - fused
+correction, -log, FDK weight and ramp filter into the device ring - and three
+arbitrarily oriented 512 x 512 slices (seeded random unit normals, offsets within
++/-10 mm) are back-projected from all 600 views in one batched launch.
+
+Metric: voxel-projection updates/s = (in-box slice pixels x views) / step time.
+  value : device time with the raw counts already resident in HBM (CUDA events)
+  e2e   : the public API with pinned host buffers (H2D of the raw counts, D2H of the
+          three images inside the timed region), host wall clock
+Multi-GPU (torchrun): every rank runs its own scan (independent objects, no
+collective on the data path); value = all ranks' updates / max-over-ranks time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(views=600, rows=384, cols=486, pixel=0.299, sod=440.0, sdd=680.0,
+                ellipsoids=40, phantom_seed=2, noise_seed=7, slice_seed=11, slices=3, n=512)
+WORKLOAD_NAME = ("cone FDK: 600 raw uint16 views 486x384 -> filtered ring -> "
+                 "3 oblique 512x512 slices in one batched launch")
+FP32_LANE_OPS_PER_UPDATE = 26       # algorithmic FP32 operations per voxel-projection update
+NOMINAL_FP32_LANE_OPS = 148 * 128 * 1965e6   # SMs x FP32 lanes x max SM clock (ops/s)
+
+
+# ------------------------------------------------------------------ workload
+def geometry():
+    from tomography_local_demo_b200 import circular_cone_vectors
+    w = WORKLOAD
+    return circular_cone_vectors(w["views"], w["sod"], w["sdd"], w["rows"], w["cols"], w["pixel"])
+
+
+def slice_requests(box):
+    rng = np.random.default_rng(WORKLOAD["slice_seed"])
+    reqs = []
+    for _ in range(WORKLOAD["slices"]):
+        nrm = rng.normal(size=3)
+        nrm /= np.linalg.norm(nrm)
+        reqs.append(dict(origin=tuple(rng.uniform(-10, 10) * nrm), normal=tuple(nrm), n=WORKLOAD["n"]))
+    return reqs
+
+
+def in_box_pixels(box, reqs):
+    from tomography_local_demo_b200.recon import slice_points
+    return [int(slice_points(box, r["origin"], r["normal"], r["n"])[1].sum()) for r in reqs]
+
+
+def make_scan(device):
+    """Raw uint16 counts [views, rows, cols] + flat/dark frames, synthesised on `device`."""
+    import torch
+    from tomography_local_demo_b200 import phantom as PH
+    w = WORKLOAD
+    geom = geometry()
+    ph = PH.EllipsoidPhantom(1.0, PH.random_ellipsoids(w["ellipsoids"], w["phantom_seed"]))
+    p = PH.project_cone_torch(ph, geom, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(w["noise_seed"])
+    shape = (w["rows"], w["cols"])
+    flat = 50000.0 * (1.0 + 0.02 * torch.randn(shape, generator=gen, device=device, dtype=torch.float64))
+    dark = 100.0 + 5.0 * torch.randn(shape, generator=gen, device=device, dtype=torch.float64)
+    raw = PH.raw_counts(p, flat, dark, seed=w["noise_seed"])
+    flats = torch.stack([torch.poisson((flat - dark).clamp(min=0), generator=gen) + dark for _ in range(4)])
+    darks = torch.stack([dark + torch.randn(shape, generator=gen, device=device, dtype=torch.float64)
+                         for _ in range(4)])
+    u16 = lambda t: t.round().clamp(0, 65535).to(torch.int32).to(torch.int16)  # noqa: E731 (uint16 bits)
+    return geom, raw.to(torch.int16), u16(flats), u16(darks)
+
+
+def as_u16(t):
+    return t.cpu().numpy().view(np.uint16)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ distributed
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl"
+        import torch
+        if not torch.cuda.is_available():
+            backend = "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world, device=None):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ CPU legs (oracle)
+def cpu_job(raw_u16, flats_u16, darks_u16, geom, reqs, box, precision="ref", pixel_stride=1,
+            view_limit=None, threads=None):
+    """The reference's CPU algorithm (oracle port): correction, FDK filter, then the
+    slices' in-box pixels (every `pixel_stride`-th) back-projected from all views.
+    Returns (images-or-values, timings dict)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import bp as obp
+    from oracle import filter as of
+    threads = threads or os.cpu_count()
+    obp.threads(threads)
+    A = raw_u16.shape[0] if view_limit is None else view_limit
+    t0 = time.perf_counter()
+    d_b = np.mean([of.bin_mean(f, 1) for f in darks_u16], axis=0)
+    f_b = np.mean([of.bin_mean(f, 1) for f in flats_u16], axis=0)
+    gain = (1.0 / np.maximum(f_b - d_b, 1.0)).astype(np.float32)
+    K = of.cone_constants(geom.vectors)
+    exact = precision == "fp64"
+
+    def chunk(i0):
+        i1 = min(A, i0 + 16)
+        x = -np.log(np.clip((raw_u16[i0:i1].astype(np.float32) - d_b) * gain, 1e-3, None))
+        Kc = {k: v[i0:i1] for k, v in K.items()}
+        return i0, of.fdk_filter_block(np.transpose(x, (1, 0, 2)), Kc, "shepp-logan", exact64=exact)
+
+    q = np.zeros((A,) + raw_u16.shape[1:], np.float64 if exact else np.float32)
+    with ThreadPoolExecutor(threads) as ex:
+        for i0, part in ex.map(chunk, range(0, A, 16)):
+            q[i0:i0 + len(part)] = part
+    t_filter = time.perf_counter() - t0
+    from oracle import geometry as og
+    vals, n_upd, t_bp = [], 0, 0.0
+    for r in reqs:
+        pts, mask = og.slice_points(box, r["origin"], r["normal"], r["n"])
+        sel = np.zeros_like(mask)
+        sel[::pixel_stride] = mask[::pixel_stride]
+        P = pts[sel]
+        t1 = time.perf_counter()
+        v = obp.bp_cone(q[:A], K["s"][:A], K["d"][:A], K["uu"][:A], K["vv"][:A], K["n"][:A],
+                        K["sdd"][:A], K["sod"][:A], P, np.pi / A)
+        t_bp += time.perf_counter() - t1
+        n_upd += len(P) * A
+        vals.append((sel, v))
+    return vals, dict(t_filter=t_filter, views=A, t_bp=t_bp, updates=n_upd, threads=threads)
+
+
+def cpu_rate(timing, total_updates, total_views):
+    """Whole-job updates/s extrapolated from a sample (filter per view, BP per update)."""
+    t_job = timing["t_filter"] / timing["views"] * total_views + timing["t_bp"] / timing["updates"] * total_updates
+    return total_updates / t_job, t_job
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank, world, local):
+    import torch
+    from tomography_local_demo_b200 import SliceReconstructor
+    from tomography_local_demo_b200.recon import KernelTimer
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    geom, raw_dev, flats, darks = make_scan(dev)
+    box = geom.volume_box()
+    reqs = slice_requests(box)
+    inbox = in_box_pixels(box, reqs)
+    V = WORKLOAD["views"]
+    updates = sum(inbox) * V
+    idx = np.arange(V)
+
+    rec = SliceReconstructor(None, geom, store=args.store, verbose=False, device=dev)
+    rec.set_flat_dark(as_u16(flats), as_u16(darks))
+    timer = KernelTimer()
+
+    def step_device():
+        rec.reset()
+        rec.add_raw_projections(idx, raw_dev)
+        return rec.reconstruct_planes_tensor(reqs)
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+    barrier(world)
+    rec.kernel_timer = timer
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        e0.record(rec.ingest_stream)
+        for _ in range(args.steps):
+            step_device()
+        e1.record(rec.stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    rec.kernel_timer = None
+    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3, world, dev)
+    kern = timer.summary()
+    launches = sum(n for n, _ in kern.values())
+
+    # ---- end to end through the public API, pinned host buffers
+    raw_host = torch.empty(raw_dev.shape, dtype=torch.int16, pin_memory=True)
+    raw_host.copy_(raw_dev)
+    rec_e = SliceReconstructor(None, geom, store=args.store, verbose=False, device=dev)
+    rec_e.set_flat_dark(as_u16(flats), as_u16(darks))
+
+    def step_e2e():
+        rec_e.reset()
+        rec_e.add_raw_projections(idx, raw_host)
+        return rec_e.reconstruct_planes(reqs)
+
+    for _ in range(args.warmup):
+        step_e2e()
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_e2e()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(time.perf_counter() - t0, world, dev)
+    h2d = raw_host.numel() * 2 + V * (64 + 32) + len(reqs) * 256
+    d2h = sum(r["n"] ** 2 for r in reqs) * 4
+
+    # ---- back-projection only: bf16 batched vs plain fp32 one request per launch
+    extra = {}
+    if rank == 0:
+        extra = bp_only_and_latency(args, dev, geom, raw_dev, flats, darks, reqs, updates, rec)
+
+    if rank != 0:
+        return None
+    ms = t_dev / args.steps * 1e3
+    value = updates * world * args.steps / t_dev
+    # roofline of the dominant kernel (largest share of device time in the timed region)
+    dom = max(kern.items(), key=lambda kv: kv[1][1])
+    line = {
+        "metric": "voxel-proj updates/s", "value": value, "unit": "updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, "views": V, "rows": WORKLOAD["rows"],
+                   "cols": WORKLOAD["cols"], "slices": len(reqs), "n": WORKLOAD["n"],
+                   "in_box_pixels": inbox, "store": args.store, "accumulate": "f32",
+                   "parallelism": f"replicas x{world}",
+                   "l2": "no flush: every step reads 224 MB raw counts and writes/reads the "
+                         f"{'224' if args.store != 'fp32' else '448'} MB ring (> 126 MB L2)"},
+        "e2e": {"value": updates * world * args.steps / t_e2e, "unit": "updates/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": t_e2e / args.steps * 1e3},
+        "gpu_launches": launches,
+        "kernels": {k: {"launches": n, "avg_ms": t / n, "share": t / sum(x[1] for x in kern.values())}
+                    for k, (n, t) in kern.items()},
+        "clocks": clocks.summary(),
+    }
+    line["roofline"] = roofline(dom[0], dom[1], updates, args.store)
+    other = [k for k in kern if k != dom[0]]
+    if other:
+        line["roofline_" + other[0]] = roofline(other[0], kern[other[0]], updates, args.store)
+    imgs = extra.pop("_images", None)
+    line.update(extra)
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"], line["accuracy"] = cpu_baseline_and_accuracy(
+            args, geom, raw_dev, flats, darks, reqs, box, updates, imgs)
+    return line
+
+
+def _traffic(kernel):
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel, {}).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def roofline(name, stats, updates, store):
+    n, t_ms = stats
+    avg = t_ms / n / 1e3
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    if name == "mr_ingest_u16":
+        w = WORKLOAD
+        out_b = 2 if store != "fp32" else 4
+        pitch = (w["cols"] + 7) // 8 * 8
+        alg = w["views"] * w["rows"] * (w["cols"] * 2 + pitch * out_b)
+        peak = peaks.get("hbm_gbs", 6650.0)
+        ach = alg / avg / 1e9
+        return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "traffic": _traffic(name), "algorithmic_bytes": alg,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    ops = updates * FP32_LANE_OPS_PER_UPDATE
+    ach = ops / avg / 1e12
+    peak = NOMINAL_FP32_LANE_OPS / 1e12
+    return {"kernel": name, "bound": "fp32-issue", "achieved": ach, "peak": peak,
+            "unit": "T FP32-lane-ops/s", "frac": ach / peak, "traffic": _traffic(name),
+            "algorithmic_ops": ops, "updates_per_s": updates / avg,
+            "peak_source": "nominal (148 SMs x 128 FP32 lanes x 1965 MHz); not in MEASURED_PEAKS.json"}
+
+
+def bp_only_and_latency(args, dev, geom, raw_dev, flats, darks, reqs, updates, rec_bf16):
+    import torch
+    from tomography_local_demo_b200 import SliceReconstructor
+    V = WORKLOAD["views"]
+    idx = np.arange(V)
+    rec32 = SliceReconstructor(None, geom, store="fp32", verbose=False, device=dev)
+    rec32.set_flat_dark(as_u16(flats), as_u16(darks))
+    rec32.add_raw_projections(idx, raw_dev)
+    reps = max(args.steps, 5)
+
+    def timed(fn, stream):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / 1e3 / reps
+
+    t32 = timed(lambda: [rec32.reconstruct_planes_tensor([r]) for r in reqs], rec32.stream)
+    rec_bf16.reset()
+    rec_bf16.add_raw_projections(idx, raw_dev)
+    tbf = timed(lambda: rec_bf16.reconstruct_planes_tensor(reqs), rec_bf16.stream)
+    t32b = timed(lambda: rec32.reconstruct_planes_tensor(reqs), rec32.stream)
+    # per-request latency of the 3-slice batch through the public API (host wall clock,
+    # includes descriptor upload and the D2H of the images)
+    lat = []
+    for i in range(50 + 5):
+        t0 = time.perf_counter()
+        rec_bf16.reconstruct_planes(reqs)
+        if i >= 5:
+            lat.append((time.perf_counter() - t0) * 1e3)
+    imgs = {"bf16": [x.cpu().numpy() for x in rec_bf16.reconstruct_planes_tensor(reqs)],
+            "fp32": [x.cpu().numpy() for x in rec32.reconstruct_planes_tensor(reqs)]}
+    return {
+        "bp_only": {"bf16_batched_updates_per_s": updates / tbf,
+                    "fp32_batched_updates_per_s": updates / t32b,
+                    "fp32_one_request_per_launch_updates_per_s": updates / t32,
+                    "bf16_batched_vs_fp32_per_request": t32 / tbf},
+        "latency_ms_3x512_batch": {"p50": float(np.percentile(lat, 50)),
+                                   "p99": float(np.percentile(lat, 99)), "samples": len(lat)},
+        "_images": imgs,
+    }
+
+
+def cpu_baseline_and_accuracy(args, geom, raw_dev, flats, darks, reqs, box, updates, imgs):
+    raw = as_u16(raw_dev)
+    fl, dk = as_u16(flats), as_u16(darks)
+    V = WORKLOAD["views"]
+    stride = 8
+    _, tm = cpu_job(raw, fl, dk, geom, reqs, box, "ref", pixel_stride=stride)
+    rate, t_job = cpu_rate(tm, updates, V)
+    base = {"value": rate, "unit": "updates/s", "cores": tm["threads"], "kind": "port",
+            "sample": (f"oracle port (C back-projection, NumPy filter) on {tm['threads']} host threads: "
+                       f"correction+filter of all {V} views ({tm['t_filter']:.2f} s) and every "
+                       f"{stride}th row of the 3 slices' in-box pixels x {V} views ({tm['t_bp']:.2f} s); "
+                       f"whole job extrapolated to {t_job:.1f} s")}
+    acc = {}
+    if imgs is not None:
+        vals64, _ = cpu_job(raw, fl, dk, geom, reqs, box, "fp64", pixel_stride=stride)
+        for store, ims in imgs.items():
+            rl, mx = [], []
+            for (sel, v64), im in zip(vals64, ims):
+                got = im[sel].astype(np.float64)
+                rl.append(float(np.linalg.norm(got - v64) / np.linalg.norm(v64)))
+                mx.append(float(np.max(np.abs(got - v64))))
+            acc[store] = {"rel_l2_vs_fp64": rl, "max_abs_err": mx}
+        acc["sample"] = f"every {stride}th row of each slice's in-box pixels"
+    return base, acc
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args, rank, world, local):
+    """The reference's CPU implementation of the path (oracle port, all host threads) on
+    the same workload, a bounded sample per step."""
+    if rank != 0:
+        return None
+    import torch
+    dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
+    geom, raw_dev, flats, darks = make_scan(dev)
+    raw, fl, dk = as_u16(raw_dev), as_u16(flats), as_u16(darks)
+    box = geom.volume_box()
+    reqs = slice_requests(box)
+    V = WORKLOAD["views"]
+    updates = sum(in_box_pixels(box, reqs)) * V
+    view_limit, stride = 96, 16          # per-step sample: 96 views filtered, 1/16 of the rows
+    for _ in range(args.warmup):
+        cpu_job(raw, fl, dk, geom, reqs, box, "ref", stride, view_limit)
+    t_jobs, tms = [], []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _, tm = cpu_job(raw, fl, dk, geom, reqs, box, "ref", stride, view_limit)
+        r, t_job = cpu_rate(tm, updates, V)
+        t_jobs.append(t_job)
+        tms.append(tm)
+    wall = time.perf_counter() - t0
+    t_job = float(np.mean(t_jobs))
+    value = updates / t_job
+    sample = (f"per step: correction+FDK filter of {view_limit} of {V} views and every {stride}th row of "
+              f"the 3 slices' in-box pixels back-projected from {view_limit} views, on "
+              f"{tms[0]['threads']} host threads; rate extrapolated to the whole job ({t_job:.1f} s)")
+    return {"metric": "voxel-proj updates/s", "value": value, "unit": "updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_job * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD_NAME, "views": V, "rows": WORKLOAD["rows"],
+                       "cols": WORKLOAD["cols"], "slices": len(reqs), "n": WORKLOAD["n"],
+                       "store": "fp32", "accumulate": "f64", "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": "updates/s", "cores": tms[0]["threads"],
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--store", choices=("fp32", "bf16", "fp16"), default="bf16")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / accuracy leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = dist_setup()
+    try:
+        line = (run_reference if args.impl == "reference" else run_ours)(args, rank, world, local)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,192 @@
+/*
+ * minirecast_b200.h - C ABI of the B200 (sm_100a) filter / back-projection library.
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t passed as
+ * `void*` (NULL = legacy default stream), allocates no device memory, and returns an
+ * int status (MR_OK = 0, negative on error). Work is enqueued on the given stream;
+ * errors found on the host (bad sizes, bad enums) are returned before anything is
+ * launched. The functions keep no state between calls except immutable tables.
+ *
+ * Conventions (the same as minirecast, the reference):
+ *   - projections are ASTRA-style; the filtered store ("ring") is [slot][row][col]
+ *     with a row pitch of `col_pitch` elements, slots in arrival order;
+ *   - detector centre at ((R-1)/2, (C-1)/2); bilinear taps outside [0,R)x[0,C) are 0;
+ *   - a cone view's sample position p projects to
+ *         col = (pu . [p,1]) / den,  row = (pv . [p,1]) / den,  den = pw . [p,1]
+ *     with den = L / SOD, and its FDK distance weight is 1/den^2 = (SOD/L)^2;
+ *     a parallel view has pw = (0,0,0,1) and weight 1.
+ */
+#ifndef MINIRECAST_B200_H
+#define MINIRECAST_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MR_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define MR_OK                0
+#define MR_ERR_INVALID      -1   /* bad argument, found on the host before any launch */
+#define MR_ERR_CUDA         -2   /* a CUDA runtime call or launch failed */
+#define MR_ERR_UNSUPPORTED  -3   /* valid but not built (e.g. FFT length out of range) */
+#define MR_ERR_TIMEOUT      -4   /* a bounded device-side wait gave up */
+
+/* ---- element types ------------------------------------------------------------- */
+#define MR_F32   0
+#define MR_BF16  1
+#define MR_F16   2
+#define MR_U16   3
+
+/* ---- beam geometry kinds ------------------------------------------------------- */
+#define MR_PARALLEL 0
+#define MR_CONE     1
+
+/* Device-resident filtered-projection store. Host struct, passed by pointer. */
+typedef struct mr_ring {
+    void*    data;          /* device pointer to slot 0, row 0, col 0 */
+    int32_t  dtype;         /* MR_F32 / MR_BF16 / MR_F16 */
+    int32_t  kind;          /* MR_PARALLEL / MR_CONE */
+    int32_t  rows;          /* R */
+    int32_t  cols;          /* C (columns >= C inside the pitch are never read) */
+    int32_t  col_pitch;     /* elements per stored row, >= C, multiple of 8 */
+    int32_t  n_slots;       /* capacity in views */
+    int64_t  slot_stride;   /* elements per slot, >= rows * col_pitch */
+} mr_ring;
+
+/* One stored view: FP32 projective map built on the host in FP64. 64 bytes. */
+typedef struct mr_view {
+    float pu[4];            /* col * den = pu . (x, y, z, 1) */
+    float pv[4];            /* row * den = pv . (x, y, z, 1) */
+    float pw[4];            /* den = pw . (x, y, z, 1) */
+    float uv;               /* row shift per column of COR shift: (u . v) / |v|^2 */
+    float qscale;           /* stored value * qscale = filtered value (1 for FP32/BF16) */
+    float pad[2];
+} mr_view;
+
+/* Sample grid of one reconstruction request. 256 bytes.
+ *   p(i,j,k) = origin + i*step_i + j*step_j + k*step_k   (mm, FP32)
+ *   out[out_offset + i*out_stride_i + j*out_stride_j + k*out_stride_k]
+ *       = scale * sum_{v < n_views} w_v(p) * bilinear(ring[v], row_v(p), col_v(p))
+ * With MR_GRID_MASK_BOX a sample is written as 0 unless the FP64 point
+ *   c + a_j*e_j + a_i*e_i,  a_x = (x - mask_half) * mask_delta
+ * lies in the box (|p_x| <= box_x for every axis), evaluated in the rounding order
+ * of minirecast slice_points (recon.py:238-265), so the mask matches it bit for bit.
+ * With MR_GRID_POINTS the positions are points[j*3 + 0..2] (n_i = n_k = 1). */
+#define MR_GRID_MASK_BOX 1
+#define MR_GRID_POINTS   2
+typedef struct mr_grid {
+    float   origin[3];
+    float   step_i[3];
+    float   step_j[3];
+    float   step_k[3];
+    float   cor_shift;      /* rotation-centre shift, detector columns */
+    float   scale;          /* pi / n_views for FBP/FDK */
+    int32_t n_i, n_j, n_k;
+    int32_t n_views;        /* use slots [0, n_views) - the snapshot at admission */
+    int32_t flags;
+    int32_t pad0;
+    int64_t out_offset;
+    int64_t out_stride_i, out_stride_j, out_stride_k;
+    const float* points;    /* device, MR_GRID_POINTS only */
+    int64_t pad1;
+    double  mask_c[3];      /* plane centre */
+    double  mask_ej[3];     /* unit vector along j (columns) */
+    double  mask_ei[3];     /* unit vector along i (rows) */
+    double  mask_half;      /* (n - 1) / 2 */
+    double  mask_delta;     /* pixel size */
+    double  box[3];         /* half sizes of the volume box */
+    int64_t pad2[2];
+} mr_grid;
+
+/* One work item of a back-projection launch: a tile of one grid. 16 bytes. */
+typedef struct mr_tile {
+    int32_t grid;           /* index into the grid array */
+    int32_t i0, j0, k;      /* first sample of the tile */
+} mr_tile;
+
+/* Per-view parameters of the ingest / filter kernels, built on the host in FP64. 32 bytes.
+ * FDK cosine weight w(r,c) = sdd / sqrt(sdd^2 + a^2 + b^2), a = a0 + c*da, b = b0 + r*db;
+ * sdd == 0 means no weight (parallel beam). The filter output is
+ *   ring[slot][r][c] = out_scale * gain * (g * (x w))[r][c]
+ * where g is the ramp kernel whose spectrum is the table H (built for tau = 1) and
+ * gain = 1 / (tau * N), N the FFT length. */
+typedef struct mr_filter_view {
+    float   a0, da, b0, db;
+    float   sdd;
+    float   gain;
+    float   out_scale;
+    int32_t slot;
+} mr_filter_view;
+
+/* ---- library information ------------------------------------------------------- */
+int         mr_abi_version(void);
+const char* mr_status_string(int status);
+/* sizeof() of the ABI structs, for layout checks by bindings:
+ * which = 0 mr_ring, 1 mr_view, 2 mr_grid, 3 mr_tile, 4 mr_filter_view; -1 otherwise. */
+int         mr_struct_size(int which);
+/* Samples per back-projection tile along i and j (host-side planning). */
+void        mr_bp_tile_shape(int32_t* tile_i, int32_t* tile_j);
+
+/* Host-only: split `n_grids` grids (host memory) into tiles (host memory).
+ * Writes at most `capacity` tiles and returns the number needed in *n_tiles. */
+int mr_plan_tiles(const mr_grid* grids_host, int32_t n_grids,
+                  mr_tile* tiles_host, int64_t capacity, int64_t* n_tiles);
+
+/* ---- back-projection ------------------------------------------------------------
+ * Replaces minirecast recon.py:193-219 (bp_cone_numba, with _bil_nb 156-173) and
+ * recon.py:175-191 (bp_parallel_numba) as called by reconstruct_points
+ * recon.py:405-424 / reconstruct_plane 426-440 / reconstruct_volume 442-470.
+ * Many grids (requests) of any size, zoom and orientation go in one launch; every
+ * sample accumulates in FP32 registers over slots [0, n_views) of its grid. */
+int mr_backproject(const mr_ring* ring, const mr_view* views_dev,
+                   const mr_grid* grids_dev, const mr_tile* tiles_dev, int64_t n_tiles,
+                   float* out_dev, void* stream);
+
+/* ---- filtering ---------------------------------------------------------------------
+ * Replaces recon.py:85-104 (fdk_filter_block) and recon.py:58-64 (filter_rows, via
+ * ramp_response 34-55) as called from add_projections recon.py:357-362.
+ * Input element (v, r, c) is block[v*s_view + r*s_row + c] (f32, device); the ASTRA
+ * block [rows, k, cols] of the reference has s_view = cols, s_row = k*cols.
+ * H: device, n_fft reals (full spectrum, mirrored), twiddle: device, n_fft complex
+ * exp(-2 pi i m / n_fft) as interleaved float pairs. n_fft = 2^log2n >= 2*cols. */
+int mr_filter_f32(const float* block, int64_t s_view, int64_t s_row,
+                  int32_t k, const mr_filter_view* views_dev,
+                  const float* H_dev, const float* twiddle_dev, int32_t log2n,
+                  const mr_ring* ring, void* stream);
+
+/* ---- fused raw ingest ----------------------------------------------------------
+ * Replaces flexray.py:111-116 + 174-184 (bin, flipud, (P-D)*gain, clip 1e-3, -log)
+ * and hdf5.py:24-31 + 73-78, fused with the filter above. Raw element (v, y, x) is
+ * raw[v*s_view + y*s_row + x] (uint16, device). Output pixel (r, c) averages raw
+ * rows [r'*bin, r'*bin+bin) x cols [c*bin, c*bin+bin) with r' = flip ? rows-1-r : r.
+ * dark, gain: device f32 [rows][cols] in output orientation, already binned:
+ *   x = -log(max((mean - dark) * gain, 1e-3)). */
+int mr_ingest_u16(const uint16_t* raw, int64_t s_view, int64_t s_row,
+                  int32_t bin, int32_t flip_rows,
+                  const float* dark_dev, const float* gain_dev,
+                  int32_t k, const mr_filter_view* views_dev,
+                  const float* H_dev, const float* twiddle_dev, int32_t log2n,
+                  const mr_ring* ring, void* stream);
+
+/* ---- pre-processing on arrival (block layout [rows, k, cols], f32, device) ------
+ * Replaces preprocess.py:31-56 (rotate_projections): every projection rotated by
+ * `degrees` about the detector centre, bilinear, zero outside. in != out. */
+int mr_rotate_f32(const float* in, float* out, int32_t rows, int32_t k, int32_t cols,
+                  double degrees, void* stream);
+
+/* Replaces one axis of preprocess.py:8-28 (gaussian_blur): edge padding by `pad`,
+ * circular convolution over the padded length with the even kernel taps[0..n_taps-1]
+ * (taps[m] = g[m] = g[-m]), crop. axis = 0 (rows) or 2 (cols). in != out. */
+int mr_gaussian_axis_f32(const float* in, float* out, int32_t rows, int32_t k, int32_t cols,
+                         int32_t axis, int32_t pad, const float* taps, int32_t n_taps,
+                         void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MINIRECAST_B200_H */

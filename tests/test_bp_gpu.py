@@ -1,0 +1,164 @@
+"""Back-projection kernel (mr_backproject) against the C oracle of minirecast's Numba
+kernels, on seeded inputs. Tolerances: FP32 store rel-L2 <= 1e-5 vs the oracle on the
+same stack; BF16/FP16 stores are checked exactly against the oracle fed the same
+rounded stack (rel-L2 <= 1e-5) and against the FP32 stack (stated bounds)."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from gpu_helpers import DeviceRing
+from oracle import bp as obp
+from oracle import filter as of
+from oracle import geometry as og
+from tomography_local_demo_b200 import _native as N
+from tomography_local_demo_b200 import recon as R
+
+pytestmark = pytest.mark.gpu
+
+
+def cone_case(A=48, rows=40, cols=56, seed=0, jitter=0.02):
+    rng = np.random.default_rng(seed)
+    V = og.circular_cone_vectors(A, 120.0, 200.0, 1.0, det_shift_u=0.6)
+    V = V + rng.normal(0.0, jitter, V.shape)
+    # smooth-ish stack: low-pass noise, like filtered projections of a phantom
+    q = rng.normal(0.0, 1.0, (A, rows, cols))
+    q = (q + np.roll(q, 1, 2) + np.roll(q, 1, 1)).astype(np.float32)
+    return V, q, rows, cols
+
+
+def oracle_cone(V, q, pts, n_views, shift=0.0):
+    K = of.cone_constants(V[:n_views])
+    D = K["d"] - shift * K["u"] if shift else K["d"]
+    return obp.bp_cone(q[:n_views], K["s"], D, K["uu"], K["vv"], K["n"], K["sdd"], K["sod"], pts,
+                       np.pi / n_views)
+
+
+@pytest.mark.parametrize("shift", [0.0, 2.3])
+def test_cone_points_match_oracle(cuda, shift):
+    V, q, rows, cols = cone_case()
+    ring = DeviceRing(q, R.cone_view_maps(R.cone_constants(V), rows, cols), N.MR_CONE)
+    rng = np.random.default_rng(1)
+    pts = rng.uniform(-22, 22, (5000, 3))
+    got = ring.points(pts, len(V), np.pi / len(V), shift)
+    want = oracle_cone(V, q, pts, len(V), shift)
+    assert rel_l2(got, want) < 1e-5
+    assert np.max(np.abs(got - want)) < 1e-4 * np.max(np.abs(want))
+
+
+def test_cone_snapshot_uses_first_n_views(cuda):
+    V, q, rows, cols = cone_case(seed=4)
+    ring = DeviceRing(q, R.cone_view_maps(R.cone_constants(V), rows, cols), N.MR_CONE)
+    pts = np.random.default_rng(2).uniform(-20, 20, (777, 3))
+    for n in (1, 7, 31):
+        got = ring.points(pts, n, np.pi / n)
+        assert rel_l2(got, oracle_cone(V, q, pts, n)) < 1e-5
+    assert np.all(ring.points(pts, 0, 0.0) == 0.0)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_cone_planes_match_oracle_with_exact_mask(cuda, seed):
+    V, q, rows, cols = cone_case(seed=seed)
+    box = og.cone_volume_box(V, rows, cols)
+    ring = DeviceRing(q, R.cone_view_maps(R.cone_constants(V), rows, cols), N.MR_CONE)
+    rng = np.random.default_rng(10 + seed)
+    reqs = []
+    for r in range(5):                 # several grids of different sizes in ONE launch
+        reqs.append(dict(origin=rng.uniform(-5, 5, 3), normal=rng.normal(size=3),
+                         n=int(rng.integers(5, 90)), zoom=float(rng.uniform(0.7, 4.0)),
+                         center=None if r % 2 else rng.uniform(-3, 3, 3),
+                         cor_shift=float(rng.uniform(-3, 3))))
+    grids = np.zeros(len(reqs), N.GRID_DTYPE)
+    off = 0
+    for r, rq in enumerate(reqs):
+        grids[r] = R.plane_grid(box, rq["origin"], rq["normal"], rq["n"], None, rq["zoom"],
+                                rq["center"], rq["cor_shift"])
+        grids[r]["out_offset"] = off
+        off += rq["n"] ** 2
+    grids["n_views"] = len(V)
+    grids["scale"] = np.pi / len(V)
+    out = ring.run(grids, off)
+    off = 0
+    for rq in reqs:
+        n = rq["n"]
+        img = out[off:off + n * n].reshape(n, n)
+        off += n * n
+        pts, mask = og.slice_points(box, rq["origin"], rq["normal"], n, None, rq["zoom"], rq["center"])
+        want = np.zeros(n * n)
+        if mask.any():
+            want[mask.ravel()] = oracle_cone(V, q, pts.reshape(-1, 3)[mask.ravel()], len(V), rq["cor_shift"])
+        want = want.reshape(n, n)
+        assert np.all(img[~mask] == 0.0)
+        if mask.any():
+            assert rel_l2(img[mask], want[mask]) < 1e-5
+
+
+def test_cone_volume_grid_matches_oracle(cuda):
+    V, q, rows, cols = cone_case(A=30, seed=7)
+    box = og.cone_volume_box(V, rows, cols)
+    ring = DeviceRing(q, R.cone_view_maps(R.cone_constants(V), rows, cols), N.MR_CONE)
+    dims, origin, h = R.volume_grid(box, 37)
+    nx, ny, nz = dims
+    grids = np.zeros(2, N.GRID_DTYPE)
+    grids[0] = R.volume_grid_record(origin, h, dims, 0, 11)      # two x-slabs, one launch
+    grids[1] = R.volume_grid_record(origin, h, dims, 11, nx)
+    grids["n_views"], grids["scale"] = len(V), np.pi / len(V)
+    vol = ring.run(grids, nx * ny * nz).reshape(nx, ny, nz)
+    x, y, z = (origin[i] + h * np.arange(dims[i]) for i in range(3))
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    want = oracle_cone(V, q, np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1), len(V)).reshape(nx, ny, nz)
+    assert rel_l2(vol, want) < 1e-5
+
+
+@pytest.mark.parametrize("shift", [0.0, -1.3])
+def test_parallel_points_and_planes_match_oracle(cuda, shift):
+    rng = np.random.default_rng(5)
+    A, rows, cols = 60, 30, 44
+    ang = np.arange(A) * np.pi / A
+    q = rng.normal(0, 1, (A, rows, cols)).astype(np.float32)
+    ring = DeviceRing(q, R.parallel_view_maps(ang, 0.9, 1.1, rows, cols), N.MR_PARALLEL)
+    pts = rng.uniform(-20, 20, (3000, 3))
+    got = ring.points(pts, A, np.pi / A, shift)
+    want = obp.bp_parallel(q, np.cos(ang), np.sin(ang), 0.9, 1.1, pts, np.pi / A, shift)
+    assert rel_l2(got, want) < 1e-5
+    box = og.parallel_volume_box(rows, cols, 0.9, 1.1)
+    g = np.zeros(1, N.GRID_DTYPE)
+    g[0] = R.plane_grid(box, (1, 2, 3), (0.2, 1.0, 0.4), 50, None, 1.3, None, shift)
+    g["n_views"], g["scale"] = A, np.pi / A
+    img = ring.run(g, 2500).reshape(50, 50)
+    pts, mask = og.slice_points(box, (1, 2, 3), (0.2, 1.0, 0.4), 50, None, 1.3, None)
+    want = obp.bp_parallel(q, np.cos(ang), np.sin(ang), 0.9, 1.1, pts.reshape(-1, 3), np.pi / A,
+                           shift).reshape(50, 50)
+    assert np.all(img[~mask] == 0)
+    assert rel_l2(img[mask], want[mask]) < 1e-5
+
+
+@pytest.mark.parametrize("store,bound", [("bf16", 5e-3), ("fp16", 1e-3)])
+def test_low_precision_stores(cuda, store, bound):
+    V, q, rows, cols = cone_case(seed=9)
+    maps = R.cone_view_maps(R.cone_constants(V), rows, cols)
+    ring = DeviceRing(q, maps, N.MR_CONE, store=store)
+    pts = np.random.default_rng(3).uniform(-20, 20, (4000, 3))
+    got = ring.points(pts, len(V), np.pi / len(V))
+    # kernel arithmetic: exact against the oracle fed the same rounded stack
+    assert rel_l2(got, oracle_cone(V, ring.stored.astype(np.float32), pts, len(V))) < 1e-5
+    # storage error against the FP32 stack (white-noise stack: the worst case)
+    assert rel_l2(got, oracle_cone(V, q, pts, len(V))) < bound
+
+
+def test_fp16_per_view_scale(cuda):
+    V, q, rows, cols = cone_case(seed=11)
+    q = q * np.linspace(1e3, 3e4, len(V))[:, None, None].astype(np.float32)   # beyond fp16 range
+    qs = 2.0 ** np.ceil(np.log2(np.abs(q).max(axis=(1, 2)) / 16384.0))
+    ring = DeviceRing(q, R.cone_view_maps(R.cone_constants(V), rows, cols), N.MR_CONE, "fp16", qs)
+    pts = np.random.default_rng(3).uniform(-20, 20, (2000, 3))
+    got = ring.points(pts, len(V), np.pi / len(V))
+    assert rel_l2(got, oracle_cone(V, q, pts, len(V))) < 1e-3
+
+
+def test_points_far_outside_detector_are_zero(cuda):
+    V, q, rows, cols = cone_case(seed=2)
+    ring = DeviceRing(q, R.cone_view_maps(R.cone_constants(V), rows, cols), N.MR_CONE)
+    pts = np.array([[500.0, 0, 0], [0, 0, 300.0], [0, 0, -300.0], [1e4, 1e4, 1e4]])
+    got = ring.points(pts, len(V), 1.0)
+    want = oracle_cone(V, q, pts, len(V)) * len(V) / np.pi
+    np.testing.assert_allclose(got, want, atol=1e-5 * max(1.0, np.abs(want).max()))

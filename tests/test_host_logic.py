@@ -1,0 +1,198 @@
+"""Host-side logic of the product (no GPU): FP64 geometry, projective maps, filter
+parameters, plane/volume grid records and the tile planner, against the oracle and the
+reference's golden vectors."""
+import numpy as np
+import pytest
+
+from conftest import golden
+from oracle import filter as of
+from oracle import geometry as og
+from tomography_local_demo_b200 import _native as N
+from tomography_local_demo_b200 import geometry as G
+from tomography_local_demo_b200 import recon as R
+from tomography_local_demo_b200 import stream as S
+
+
+def test_ramp_response_matches_reference():
+    g = golden("ramp.npz")
+    for key, H in g.items():
+        _, n, tau, w = key.split("_", 3)
+        Hp, N_ = R.ramp_response(int(n), float(tau), w)
+        assert N_ == len(H)
+        np.testing.assert_allclose(Hp, H, rtol=0, atol=1e-12 * np.abs(H).max())
+    with pytest.raises(ValueError):
+        R.ramp_response(16, 1.0, "bogus")
+
+
+def test_geometry_containers_match_reference():
+    g = golden("phantom.npz")
+    cg = G.circular_cone_vectors(9, 300.0, 600.0, 10, 12, 15.0, det_shift_u=1.5)
+    np.testing.assert_allclose(cg.vectors, g["cone_V"], rtol=1e-15, atol=1e-12)
+    np.testing.assert_allclose(cg.volume_box(), og.cone_volume_box(cg.vectors, 10, 12), rtol=1e-15)
+    pg = G.ParallelGeometry(np.arange(9) * np.pi / 9, 10, 12, 9.0, 11.0)
+    np.testing.assert_allclose(pg.volume_box(), og.parallel_volume_box(10, 12, 9.0, 11.0))
+    assert pg.n_angles == 9 and cg.n_angles == 9
+    fg = golden("fdk.npz")
+    K = R.cone_constants(fg["V_gen"])
+    for k in K:
+        np.testing.assert_allclose(K[k], fg["K_" + k], rtol=1e-14, atol=1e-12)
+
+
+def _ref_project(K, k, p, rows, cols, shift=0.0):
+    """recon.py:206-217 in float64 for one view and points p [M,3]."""
+    D = K["d"][k] - shift * K["u"][k]
+    rel = p - K["s"][k]
+    L = rel @ K["n"][k]
+    t = K["sdd"][k] / L
+    X = K["s"][k] + t[:, None] * rel - D
+    return (X @ K["vv"][k] + (rows - 1) / 2.0, X @ K["uu"][k] + (cols - 1) / 2.0,
+            (K["sod"][k] / L) ** 2)
+
+
+@pytest.mark.parametrize("shift", [0.0, 1.7, -3.2])
+def test_cone_view_maps_reproduce_reference_projection(shift):
+    fg = golden("fdk.npz")
+    V = fg["V_gen"]
+    rows, cols = 16, 20
+    K = R.cone_constants(V)
+    maps = R.cone_view_maps(K, rows, cols)
+    rng = np.random.default_rng(3)
+    p = rng.uniform(-20, 20, (50, 3))
+    ph = np.concatenate([p, np.ones((50, 1))], 1)
+    for k in range(len(V)):
+        pu = maps["pu"][k].astype(np.float64) + shift * maps["pw"][k]
+        pv = maps["pv"][k].astype(np.float64) + shift * maps["uv"][k] * maps["pw"][k]
+        den = ph @ maps["pw"][k].astype(np.float64)
+        row_r, col_r, w_r = _ref_project(K, k, p, rows, cols, shift)
+        # FP32-rounded map coefficients: agreement to ~1e-5 detector pixels
+        np.testing.assert_allclose((ph @ pu) / den, col_r, atol=2e-4)
+        np.testing.assert_allclose((ph @ pv) / den, row_r, atol=2e-4)
+        np.testing.assert_allclose(1.0 / den ** 2, w_r, rtol=1e-5)
+
+
+def test_parallel_view_maps():
+    a = np.array([0.0, 0.3, 2.0])
+    maps = R.parallel_view_maps(a, 0.9, 1.1, 16, 20)
+    p = np.array([[1.0, -2.0, 3.0], [0.5, 0.25, -4.0]])
+    ph = np.concatenate([p, np.ones((2, 1))], 1)
+    for k in range(3):
+        col = (-p[:, 0] * np.sin(a[k]) + p[:, 1] * np.cos(a[k])) / 0.9 + 9.5
+        np.testing.assert_allclose(ph @ maps["pu"][k].astype(np.float64), col, atol=1e-5)
+        np.testing.assert_allclose(ph @ maps["pv"][k].astype(np.float64), p[:, 2] / 1.1 + 7.5, atol=1e-5)
+        assert tuple(maps["pw"][k]) == (0, 0, 0, 1)
+
+
+def test_cone_filter_views_reproduce_fdk_weight():
+    fg = golden("fdk.npz")
+    K = R.cone_constants(fg["V_gen"])
+    rows, cols = 16, 20
+    fv = R.cone_filter_views(K, rows, cols, 64, np.arange(7))
+    cc = np.arange(cols) - (cols - 1) / 2.0
+    rr = np.arange(rows) - (rows - 1) / 2.0
+    for k in range(7):
+        s, d, u, v, n = (K[x][k] for x in ("s", "d", "u", "v", "n"))
+        sdd, sod = K["sdd"][k], K["sod"][k]
+        off = d - (s + sdd * n)
+        un, vn = np.linalg.norm(u), np.linalg.norm(v)
+        a = off @ u / un + cc * un
+        b = off @ v / vn + rr * vn
+        w_ref = sdd / np.sqrt(sdd ** 2 + a[None, :] ** 2 + b[:, None] ** 2)
+        a2 = fv["a0"][k] + np.arange(cols) * fv["da"][k]
+        b2 = fv["b0"][k] + np.arange(rows) * fv["db"][k]
+        w2 = fv["sdd"][k] / np.sqrt(fv["sdd"][k] ** 2 + a2[None, :] ** 2 + b2[:, None] ** 2)
+        np.testing.assert_allclose(w2, w_ref, rtol=1e-6)
+        np.testing.assert_allclose(1.0 / (fv["gain"][k] * 64), un * sod / sdd, rtol=1e-6)
+
+
+def _device_mask(g):
+    """The FP64 mask formula of bp.cu:in_box_fp64, evaluated in NumPy with the same
+    operation order (no fused multiply-add)."""
+    n_i, n_j = int(g["n_i"]), int(g["n_j"])
+    aj = (np.arange(n_j) - g["mask_half"]) * g["mask_delta"]
+    ai = (np.arange(n_i) - g["mask_half"]) * g["mask_delta"]
+    ok = np.ones((n_i, n_j), bool)
+    for e in range(3):
+        p = (g["mask_c"][e] + aj[None, :] * g["mask_ej"][e]) + ai[:, None] * g["mask_ei"][e]
+        ok &= np.abs(p) <= g["box"][e]
+    return ok
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_plane_grid_mask_and_points_match_slice_points(seed):
+    rng = np.random.default_rng(seed)
+    box = np.array([47.0, 47.0, 37.2]) * rng.uniform(0.5, 1.5)
+    normal = rng.normal(size=3)
+    origin = rng.uniform(-10, 10, 3)
+    n = int(rng.integers(16, 200))
+    zoom = float(rng.uniform(0.5, 3.0))
+    center = None if seed % 2 else rng.uniform(-5, 5, 3)
+    g = R.plane_grid(box, origin, normal, n, None, zoom, center)
+    pts, mask = og.slice_points(box, origin, normal, n, None, zoom, center)
+    np.testing.assert_array_equal(_device_mask(g), mask)
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    p32 = (g["origin"].astype(np.float64) + i[..., None] * g["step_i"].astype(np.float64)
+           + j[..., None] * g["step_j"].astype(np.float64))
+    np.testing.assert_allclose(p32, pts, atol=1e-4 * max(1.0, np.abs(pts).max()))
+
+
+def test_axis_aligned_plane_masks():
+    box = np.array([47.0, 47.0, 37.2])
+    for normal in ((0, 0, 1), (0, 1, 0), (1, 0, 0), (1, 1, 0)):
+        for n in (1, 2, 64, 511, 512):
+            g = R.plane_grid(box, (0, 0, 0), normal, n)
+            _, mask = og.slice_points(box, (0, 0, 0), normal, n)
+            np.testing.assert_array_equal(_device_mask(g), mask)
+
+
+def test_volume_grid_record_positions():
+    dims, origin, h = R.volume_grid(np.array([10.0, 12.0, 7.0]), 16)
+    d2, o2, h2 = og.volume_points(np.array([10.0, 12.0, 7.0]), maxdim=16)
+    np.testing.assert_array_equal(dims, d2)
+    np.testing.assert_allclose(origin, o2)
+    assert h == h2
+    g = R.volume_grid_record(origin, h, dims, 2, 5)
+    nx, ny, nz = dims
+    assert (g["n_i"], g["n_j"], g["n_k"]) == (ny, nz, 3)
+    assert g["out_offset"] == 2 * ny * nz
+    # sample (i=y, j=z, k) sits at (x[2+k], y[i], z[j])
+    p = g["origin"] + 1 * g["step_k"] + 3 * g["step_i"] + 4 * g["step_j"]
+    np.testing.assert_allclose(p, origin + h * np.array([3, 3, 4]), atol=1e-5)
+
+
+def test_tile_planner_covers_every_sample():
+    grids = np.zeros(3, dtype=N.GRID_DTYPE)
+    grids["n_i"], grids["n_j"], grids["n_k"] = [100, 1, 33], [70, 5000, 40], [1, 1, 3]
+    grids["flags"][1] = N.MR_GRID_POINTS
+    tiles = N.plan_tiles(grids)
+    ti, tj = N.tile_shape()
+    cover = {0: set(), 2: set()}
+    pts = set()
+    for t in tiles:
+        if t["grid"] == 1:
+            pts.update(range(t["j0"], min(5000, t["j0"] + ti * tj // 4 * 4)))
+            continue
+        G_ = grids[t["grid"]]
+        for i in range(t["i0"], min(G_["n_i"], t["i0"] + ti)):
+            for j in range(t["j0"], min(G_["n_j"], t["j0"] + tj)):
+                cover[t["grid"]].add((i, j, t["k"]))
+    assert len(cover[0]) == 100 * 70 and len(cover[2]) == 33 * 40 * 3
+    assert pts == set(range(5000))
+    assert len(N.plan_tiles(np.zeros(0, dtype=N.GRID_DTYPE))) == 0
+
+
+def test_filter_tables_mirror_the_rfft_half():
+    H, n_fft = R.ramp_response(486, 1.0, "shepp-logan")
+    half = H[: n_fft // 2 + 1]
+    full = np.concatenate([half, half[1:n_fft - n_fft // 2][::-1]])
+    assert len(full) == n_fft == 1024
+    np.testing.assert_array_equal(full[: n_fft // 2 + 1], half)
+    np.testing.assert_array_equal(full[n_fft - np.arange(1, n_fft // 2)], half[1:n_fft // 2])
+
+
+def test_stream_arrival_order_matches_reference():
+    g = golden("misc.npz")
+    for n in (1, 2, 10, 17, 64, 600):
+        np.testing.assert_array_equal(S.arrival_order(n, "interleaved"), g[f"order_{n}"])
+    np.testing.assert_array_equal(S.arrival_order(5), np.arange(5))
+    with pytest.raises(ValueError):
+        S.arrival_order(5, "random")

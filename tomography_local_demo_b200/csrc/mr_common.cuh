@@ -1,0 +1,45 @@
+// Shared device helpers of the sm_100a filter / back-projection library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+#include "minirecast_b200.h"
+
+#define MR_CUDA_TRY(expr)                                  \
+    do {                                                   \
+        cudaError_t e_ = (expr);                           \
+        if (e_ != cudaSuccess) return MR_ERR_CUDA;         \
+    } while (0)
+
+namespace mr {
+
+// Stored-element loads through the read-only path, widened to FP32.
+__device__ __forceinline__ float ld_elem(const float* p) { return __ldg(p); }
+__device__ __forceinline__ float ld_elem(const __nv_bfloat16* p) {
+    const unsigned short u = __ldg(reinterpret_cast<const unsigned short*>(p));
+    return __uint_as_float(static_cast<unsigned>(u) << 16);
+}
+__device__ __forceinline__ float ld_elem(const __half* p) { return __half2float(__ldg(p)); }
+
+// Stored-element writes from FP32 (round to nearest even).
+__device__ __forceinline__ void st_elem(float* p, float v) { *p = v; }
+__device__ __forceinline__ void st_elem(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+__device__ __forceinline__ void st_elem(__half* p, float v) { *p = __float2half_rn(v); }
+
+// Fast reciprocal (PTX rcp.approx: at most 1 ulp from the correctly rounded value).
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+}  // namespace mr

@@ -1,0 +1,823 @@
+"""On-demand slice reconstruction on one B200: the drop-in for minirecast recon.py.
+
+Projections are filtered on arrival (FBP / FDK row filter, sm_100a FFT kernel) into a
+device-resident ring of filtered views; any slice, point set or volume is then
+back-projected on demand by the sm_100a voxel-driven kernel from every view received
+so far. The public surface (module functions and `SliceReconstructor`) follows
+minirecast recon.py:34-519 name for name; NumPy in, NumPy out, with torch-tensor
+variants for device-resident callers.
+
+FP64 is used on the host only, to build the per-view projective maps and the filter
+spectrum (as the reference does); the device computes in FP32 and stores the filtered
+views in FP32 (default), BF16 or FP16.
+"""
+import threading
+import time
+
+import numpy as np
+import torch
+
+from . import _native as N
+from . import preprocess
+from .geometry import ConeVecGeometry, ParallelGeometry
+
+HAVE_CUDA = True
+BACKEND = "cuda-sm100a"
+
+_STORE_DTYPES = {"fp32": (N.MR_F32, torch.float32), "bf16": (N.MR_BF16, torch.bfloat16),
+                 "fp16": (N.MR_F16, torch.float16)}
+
+
+# --------------------------------------------------------------------------
+# Filter spectrum (host, FP64) - recon.py:34-55
+# --------------------------------------------------------------------------
+def ramp_response(n, tau, window="shepp-logan"):
+    """Spectrum of the discrete Ram-Lak kernel (Kak & Slaney), zero-padded to
+    N = 2^ceil(log2(2n)), times an optional apodisation window. Returns (H, N)."""
+    N_fft = int(2 ** np.ceil(np.log2(2 * n)))
+    m = np.fft.fftfreq(N_fft, d=1.0 / N_fft).astype(np.int64)     # 0..N/2-1, -N/2..-1
+    h = np.zeros(N_fft)
+    h[0] = 1.0 / (4.0 * tau * tau)
+    odd = m % 2 == 1
+    h[odd] = -1.0 / (np.pi * m[odd] * tau) ** 2
+    H = np.real(np.fft.fft(h)) * tau
+    f = np.fft.fftfreq(N_fft)
+    if window in (None, "ram-lak", "none"):
+        pass
+    elif window == "shepp-logan":
+        H *= np.sinc(f)
+    elif window == "hann":
+        H *= 0.5 * (1.0 + np.cos(2.0 * np.pi * f))
+    elif window == "cosine":
+        H *= np.cos(np.pi * f)
+    else:
+        raise ValueError(f"unknown filter window {window!r}")
+    return H, N_fft
+
+
+class _FilterTables:
+    """Device copies of the tau = 1 spectrum (mirrored from the rfft half, exactly the
+    bins irfft uses) and of the FFT twiddles, for one detector width and window."""
+
+    def __init__(self, cols, window, device):
+        H, n_fft = ramp_response(cols, 1.0, window)
+        half = H[: n_fft // 2 + 1]
+        full = np.concatenate([half, half[1:n_fft - n_fft // 2][::-1]])
+        tw = np.exp(-2j * np.pi * np.arange(n_fft) / n_fft)
+        self.n_fft = n_fft
+        self.log2n = int(round(np.log2(n_fft)))
+        self.H = torch.from_numpy(full.astype(np.float32)).to(device)
+        self.tw = torch.from_numpy(np.stack([tw.real, tw.imag], 1).astype(np.float32)).to(device)
+
+
+# --------------------------------------------------------------------------
+# Per-view constants (host, FP64) - recon.py:70-82
+# --------------------------------------------------------------------------
+def cone_constants(vectors):
+    """Per view: src, det, u, v, u/|u|^2, v/|v|^2, unit normal oriented source ->
+    detector, source-detector-plane distance SDD and source-axis distance SOD."""
+    V = np.asarray(vectors, dtype=np.float64)
+    s, d, u, v = V[:, 0:3], V[:, 3:6], V[:, 6:9], V[:, 9:12]
+    n = np.cross(u, v)
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    n *= np.sign(np.einsum("ij,ij->i", d - s, n))[:, None]
+    sdd = np.einsum("ij,ij->i", d - s, n)
+    sod = np.einsum("ij,ij->i", -s, n)
+    uu = u / np.einsum("ij,ij->i", u, u)[:, None]
+    vv = v / np.einsum("ij,ij->i", v, v)[:, None]
+    return dict(s=s, d=d, u=u, v=v, uu=uu, vv=vv, n=n, sdd=sdd, sod=sod)
+
+
+def cone_view_maps(K, rows, cols, qscale=None):
+    """FP64 projective maps of cone views -> mr_view records (FP32).
+
+    With L = (p - s).n, t = SDD/L and X = s + t (p - s) - d (recon.py:206-215):
+    col = X.uu + (C-1)/2 = (pu.[p,1]) / den, row likewise, den = L / SOD, so the FDK
+    weight (SOD/L)^2 is 1/den^2."""
+    s, d, n, uu, vv = K["s"], K["d"], K["n"], K["uu"], K["vv"]
+    sdd, sod = K["sdd"][:, None], K["sod"][:, None]
+    e_u = np.einsum("ij,ij->i", s - d, uu)[:, None] + (cols - 1) / 2.0
+    e_v = np.einsum("ij,ij->i", s - d, vv)[:, None] + (rows - 1) / 2.0
+    n_s = np.einsum("ij,ij->i", n, s)[:, None]
+    out = np.zeros(len(s), dtype=N.VIEW_DTYPE)
+    pu = np.concatenate([(e_u * n + sdd * uu) / sod,
+                         -(e_u * n_s + sdd * np.einsum("ij,ij->i", uu, s)[:, None]) / sod], 1)
+    pv = np.concatenate([(e_v * n + sdd * vv) / sod,
+                         -(e_v * n_s + sdd * np.einsum("ij,ij->i", vv, s)[:, None]) / sod], 1)
+    pw = np.concatenate([n / sod, -n_s / sod], 1)
+    out["pu"], out["pv"], out["pw"] = pu, pv, pw
+    out["uv"] = np.einsum("ij,ij->i", K["u"], vv)
+    out["qscale"] = 1.0 if qscale is None else qscale
+    return out
+
+
+def parallel_view_maps(angles, pixel_u, pixel_v, rows, cols, qscale=None):
+    """Affine maps of parallel views (recon.py:185-188): col = (-x sin + y cos)/pu +
+    (C-1)/2, row = z/pv + (R-1)/2, den = 1."""
+    a = np.asarray(angles, dtype=np.float64)
+    out = np.zeros(len(a), dtype=N.VIEW_DTYPE)
+    out["pu"][:, 0] = -np.sin(a) / pixel_u
+    out["pu"][:, 1] = np.cos(a) / pixel_u
+    out["pu"][:, 3] = (cols - 1) / 2.0
+    out["pv"][:, 2] = 1.0 / pixel_v
+    out["pv"][:, 3] = (rows - 1) / 2.0
+    out["pw"][:, 3] = 1.0
+    out["qscale"] = 1.0 if qscale is None else qscale
+    return out
+
+
+def cone_filter_views(K, rows, cols, n_fft, slots, out_scale=1.0):
+    """mr_filter_view records of cone views (fdk_filter_block, recon.py:93-103)."""
+    s, d, u, v, n = K["s"], K["d"], K["u"], K["v"], K["n"]
+    sdd, sod = K["sdd"], K["sod"]
+    off = d - (s + sdd[:, None] * n)
+    un, vn = np.linalg.norm(u, axis=1), np.linalg.norm(v, axis=1)
+    fv = np.zeros(len(s), dtype=N.FILTER_VIEW_DTYPE)
+    fv["a0"] = np.einsum("ij,ij->i", off, u) / un - (cols - 1) / 2.0 * un
+    fv["da"] = un
+    fv["b0"] = np.einsum("ij,ij->i", off, v) / vn - (rows - 1) / 2.0 * vn
+    fv["db"] = vn
+    fv["sdd"] = sdd
+    tau = un * sod / sdd
+    fv["gain"] = 1.0 / (tau * n_fft)
+    fv["out_scale"] = out_scale
+    fv["slot"] = slots
+    return fv
+
+
+def parallel_filter_views(pixel_u, k, n_fft, slots, out_scale=1.0):
+    fv = np.zeros(k, dtype=N.FILTER_VIEW_DTYPE)
+    fv["gain"] = 1.0 / (pixel_u * n_fft)
+    fv["out_scale"] = out_scale
+    fv["slot"] = slots
+    return fv
+
+
+# --------------------------------------------------------------------------
+# Device helpers
+# --------------------------------------------------------------------------
+def _device(device=None):
+    if not torch.cuda.is_available():
+        raise RuntimeError("a CUDA device is required: this library has no CPU path")
+    return torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+
+
+def ctypes_void(x):
+    import ctypes
+    return ctypes.c_void_p(int(x))
+
+
+def _ring_struct(ring_tensor, dtype_code, kind, rows, cols):
+    r = N.MrRing()
+    r.data = ring_tensor.data_ptr()
+    r.dtype = dtype_code
+    r.kind = kind
+    r.rows = rows
+    r.cols = cols
+    r.col_pitch = ring_tensor.shape[2]
+    r.n_slots = ring_tensor.shape[0]
+    r.slot_stride = ring_tensor.shape[1] * ring_tensor.shape[2]
+    return r
+
+
+def _to_device_tensor(arr, device, dtype=None):
+    if isinstance(arr, torch.Tensor):
+        t = arr
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(arr))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.to(device, non_blocking=True).contiguous()
+
+
+def _struct_tensor(records, device):
+    raw = np.ascontiguousarray(records).view(np.uint8)
+    return torch.from_numpy(raw.copy()).to(device, non_blocking=False)
+
+
+def filter_block_device(block, s_view, s_row, k, fviews_dev, tables, ring, stream):
+    """Filter k views of a device f32 block into ring slots (mr_filter_f32)."""
+    lib = N.load()
+    st = lib.mr_filter_f32(ctypes_void(block.data_ptr()), s_view, s_row, k,
+                           ctypes_void(fviews_dev.data_ptr()), ctypes_void(tables.H.data_ptr()),
+                           ctypes_void(tables.tw.data_ptr()), tables.log2n, ring,
+                           ctypes_void(stream.cuda_stream))
+    N.check(st, "mr_filter_f32")
+
+
+class KernelTimer:
+    """CUDA events recorded right around each library launch, on the launch's stream."""
+
+    def __init__(self):
+        self.records = []
+
+    def start(self, stream):
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(stream)
+        return ev
+
+    def stop(self, name, ev0, stream):
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev1.record(stream)
+        self.records.append((name, ev0, ev1))
+
+    def summary(self):
+        """{name: (launches, total ms)} of everything recorded so far."""
+        torch.cuda.synchronize()
+        out = {}
+        for name, a, b in self.records:
+            n, t = out.get(name, (0, 0.0))
+            out[name] = (n + 1, t + a.elapsed_time(b))
+        return out
+
+    def clear(self):
+        self.records = []
+
+
+def backproject_device(ring, views_dev, grids, out, stream, device, timer=None):
+    """Back-project numpy GRID_DTYPE records into the device f32 tensor `out`."""
+    tiles = N.plan_tiles(grids)
+    if len(tiles) == 0:
+        return
+    g_dev = _struct_tensor(grids, device)
+    t_dev = _struct_tensor(tiles, device)
+    lib = N.load()
+    ev0 = timer.start(stream) if timer is not None else None
+    st = lib.mr_backproject(ring, ctypes_void(views_dev.data_ptr()), ctypes_void(g_dev.data_ptr()),
+                            ctypes_void(t_dev.data_ptr()), len(tiles), ctypes_void(out.data_ptr()),
+                            ctypes_void(stream.cuda_stream))
+    if timer is not None:
+        timer.stop("mr_backproject", ev0, stream)
+    N.check(st, "mr_backproject")
+    # keep the descriptor tensors alive until the kernel has consumed them
+    g_dev.record_stream(stream)
+    t_dev.record_stream(stream)
+
+
+# --------------------------------------------------------------------------
+# Stand-alone filter functions (recon.py:58-64, 85-104), run on the GPU
+# --------------------------------------------------------------------------
+def _filter_generic(data3, fviews, cols, window, device):
+    """data3: [k, R, C] f32 -> [k, R, C] f32 filtered on the device."""
+    dev = _device(device)
+    k, R, C = data3.shape
+    tables = _FilterTables(C, window, dev)
+    pitch = (C + 7) // 8 * 8
+    with torch.cuda.device(dev):
+        stream = torch.cuda.current_stream(dev)
+        x = _to_device_tensor(np.ascontiguousarray(data3, dtype=np.float32), dev)
+        out = torch.empty((k, R, pitch), dtype=torch.float32, device=dev)
+        ring = _ring_struct(out, N.MR_F32, N.MR_PARALLEL, R, C)
+        fv = fviews(tables.n_fft)
+        fv_dev = _struct_tensor(fv, dev)
+        for v0 in range(0, k, 65535):
+            kk = min(65535, k - v0)
+            sub = x[v0:v0 + kk]
+            fv_sub = fv_dev[v0 * N.FILTER_VIEW_DTYPE.itemsize:(v0 + kk) * N.FILTER_VIEW_DTYPE.itemsize]
+            filter_block_device(sub, R * C, C, kk, fv_sub, tables, ring, stream)
+        res = out[:, :, :C].cpu().numpy()
+    return res
+
+
+def filter_rows(data, tau, window="shepp-logan"):
+    """Ramp-filter along the last axis (any leading shape), FP32 FFT on the device."""
+    a = np.asarray(data, dtype=np.float32)
+    shape = a.shape
+    C = shape[-1]
+    flat = a.reshape(-1, 1, C)
+    k = flat.shape[0]
+    res = _filter_generic(flat, lambda n_fft: parallel_filter_views(tau, k, n_fft, np.arange(k)),
+                          C, window, None)
+    return res.reshape(shape)
+
+
+def fdk_filter_block(block, K, window="shepp-logan"):
+    """FDK cosine pre-weight + ramp filter of block [rows, k, cols] -> [k, rows, cols]."""
+    b = np.asarray(block, dtype=np.float32)
+    R, A, C = b.shape
+    data3 = np.ascontiguousarray(np.transpose(b, (1, 0, 2)))
+    return _filter_generic(data3, lambda n_fft: cone_filter_views(K, R, C, n_fft, np.arange(A)),
+                           C, window, None)
+
+
+# --------------------------------------------------------------------------
+# Plane helpers (host, FP64) - recon.py:225-283
+# --------------------------------------------------------------------------
+def plane_basis(normal):
+    n = np.asarray(normal, dtype=float)
+    n = n / np.linalg.norm(n)
+    z = np.array([0.0, 0.0, 1.0])
+    e1 = np.cross(z, n) if abs(n @ z) < 0.9 else np.cross(n, np.array([0.0, 1.0, 0.0]))
+    e1 /= np.linalg.norm(e1)
+    return n, e1, np.cross(n, e1)
+
+
+def plane_points(origin, normal, size, n):
+    """n x n points (mm) of a square of side `size`: rows follow e2, columns e1."""
+    _, e1, e2 = plane_basis(normal)
+    t = (np.arange(n) - (n - 1) / 2.0) * (size / n)
+    a, b = np.meshgrid(t, t, indexing="xy")
+    return np.asarray(origin, float) + a[..., None] * e1 + b[..., None] * e2
+
+
+def plane_size_for_box(box, normal):
+    _, e1, e2 = plane_basis(normal)
+    return 2.0 * float(max(np.abs(e1) @ box, np.abs(e2) @ box))
+
+
+def _plane_frame(box, origin, normal, n, size, zoom, center):
+    """(centre on the plane, e1, e2, size) as computed by slice_points."""
+    n_hat = np.asarray(normal, float) / np.linalg.norm(normal)
+    o = np.asarray(origin, float)
+    c = np.zeros(3) if center is None else np.asarray(center, float)
+    o = c - ((c - o) @ n_hat) * n_hat
+    if size is None:
+        size = plane_size_for_box(box, normal) / max(float(zoom), 1e-6)
+    _, e1, e2 = plane_basis(normal)
+    return o, e1, e2, float(size)
+
+
+def slice_points(box, origin, normal, n=256, size=None, zoom=1.0, center=None):
+    """Points of an n x n slice and its in-box mask (recon.py:253-265)."""
+    o, _, _, size = _plane_frame(box, origin, normal, n, size, zoom, center)
+    pts = plane_points(o, normal, size, n)
+    mask = np.all(np.abs(pts) <= box, axis=-1)
+    return pts, mask
+
+
+def planes_intersection(normals, origins, fallback=(0.0, 0.0, 0.0)):
+    N_ = np.asarray(normals, float)
+    N_ = N_ / np.linalg.norm(N_, axis=1, keepdims=True)
+    b = np.einsum("ij,ij->i", N_, np.asarray(origins, float))
+    if np.linalg.matrix_rank(N_, tol=1e-3) < 3:
+        return np.asarray(fallback, float)
+    return np.linalg.lstsq(N_, b, rcond=None)[0]
+
+
+def volume_grid(box, maxdim):
+    h = 2.0 * float(np.max(box)) / maxdim
+    dims = np.maximum(np.ceil(2.0 * np.asarray(box) / h).astype(int), 2)
+    origin = -np.asarray(box) + h / 2.0
+    return dims, origin, h
+
+
+def plane_grid(box, origin, normal, n, size=None, zoom=1.0, center=None, cor_shift=0.0):
+    """One mr_grid record for an n x n slice (masked to the box), output offset 0."""
+    o, e1, e2, size = _plane_frame(box, origin, normal, n, size, zoom, center)
+    g = np.zeros(1, dtype=N.GRID_DTYPE)[0]
+    delta = size / n
+    half = (n - 1) / 2.0
+    t0 = -half * delta
+    g["origin"] = o + t0 * e1 + t0 * e2
+    g["step_i"] = delta * e2
+    g["step_j"] = delta * e1
+    g["cor_shift"] = cor_shift
+    g["n_i"], g["n_j"], g["n_k"] = n, n, 1
+    g["flags"] = N.MR_GRID_MASK_BOX
+    g["out_stride_i"], g["out_stride_j"] = n, 1
+    g["mask_c"], g["mask_ej"], g["mask_ei"] = o, e1, e2
+    g["mask_half"], g["mask_delta"] = half, delta
+    g["box"] = box
+    return g
+
+
+def volume_grid_record(origin, h, dims, k0=0, k1=None):
+    """mr_grid record of a regular volume [nx, ny, nz] (x slowest, z fastest), for the
+    x planes [k0, k1): samples (i=y, j=z, k=x)."""
+    nx, ny, nz = (int(d) for d in dims)
+    k1 = nx if k1 is None else k1
+    g = np.zeros(1, dtype=N.GRID_DTYPE)[0]
+    g["origin"] = [origin[0] + h * k0, origin[1], origin[2]]
+    g["step_i"] = [0.0, h, 0.0]
+    g["step_j"] = [0.0, 0.0, h]
+    g["step_k"] = [h, 0.0, 0.0]
+    g["n_i"], g["n_j"], g["n_k"] = ny, nz, k1 - k0
+    g["out_offset"] = k0 * ny * nz
+    g["out_stride_i"], g["out_stride_j"], g["out_stride_k"] = nz, 1, ny * nz
+    return g
+
+
+# --------------------------------------------------------------------------
+# Public reconstructor (recon.py:289-519)
+# --------------------------------------------------------------------------
+class SliceReconstructor:
+    """Filter projections as they arrive, then reconstruct any slice on demand.
+
+    proj     : optional [rows, angles, cols] array with ALL projections (batch mode);
+               omit it and call add_projections() to stream data in (live mode).
+    gaussian : sigma (detector pixels) of a Gaussian low-pass on each projection.
+    tilt     : detector tilt correction in degrees (rotates each projection).
+    store    : filtered-view storage, "fp32" (default), "bf16" or "fp16".
+    device   : CUDA device (default: the current one).
+    The `backend` argument is accepted for compatibility; the backend is always
+    "cuda-sm100a".
+    """
+
+    def __init__(self, proj=None, geom=None, window="shepp-logan", backend="auto",
+                 gaussian=0.0, tilt=0.0, verbose=True, store="fp32", device=None):
+        if geom is None:
+            raise ValueError("geometry is required")
+        if store not in _STORE_DTYPES:
+            raise ValueError(f"unknown store {store!r}: use one of {sorted(_STORE_DTYPES)}")
+        self.device = _device(device)
+        N.load()
+        self.requested_backend = backend
+        self.backend = BACKEND
+        self.geom = geom
+        self.window = window
+        self.gaussian = float(gaussian)
+        self.tilt = float(tilt)
+        self.verbose = verbose
+        self.store = store
+        self.box = np.asarray(geom.volume_box(), dtype=float)
+        self.n_total = geom.n_angles
+        self.cor_shift = 0.0
+        self.version = 0
+        self._lock = threading.RLock()
+        self._ingest_lock = threading.Lock()
+        self._order = np.zeros(self.n_total, dtype=np.int64)
+        self._received = np.zeros(self.n_total, dtype=bool)
+        self.n = 0
+        R, C = geom.rows, geom.cols
+        self._dtype_code, tdtype = _STORE_DTYPES[store]
+        self._pitch = (C + 7) // 8 * 8
+
+        if isinstance(geom, ParallelGeometry):
+            self.kind = "parallel"
+            self._kind_code = N.MR_PARALLEL
+            self._maps_all = parallel_view_maps(geom.angles, geom.pixel_u, geom.pixel_v, R, C)
+        elif isinstance(geom, ConeVecGeometry):
+            self.kind = "cone"
+            self._kind_code = N.MR_CONE
+            self._K_all = cone_constants(geom.vectors)
+            self._maps_all = cone_view_maps(self._K_all, R, C)
+            if geom.angular_range < 2 * np.pi - 1e-3 and verbose:
+                print("note: short scan (<360 deg) - no Parker weights, expect some artefacts")
+        else:
+            raise TypeError(type(geom))
+        ramp_response(C, 1.0, window)          # validates the window name early
+
+        with torch.cuda.device(self.device):
+            self.stream = torch.cuda.Stream(self.device)          # reconstruction
+            self.ingest_stream = torch.cuda.Stream(self.device)   # filtering of new views
+            self._tables = _FilterTables(C, window, self.device)
+            self._ring = torch.zeros((self.n_total, R, self._pitch), dtype=tdtype, device=self.device)
+            self._views_host = np.zeros(self.n_total, dtype=N.VIEW_DTYPE)
+            self._views_dev = torch.zeros(self.n_total * N.VIEW_DTYPE.itemsize, dtype=torch.uint8,
+                                          device=self.device)
+        self._ring_c = _ring_struct(self._ring, self._dtype_code, self._kind_code, R, C)
+        self._ingest_event = None
+        self.kernel_timer = None        # a KernelTimer records launch durations when set
+
+        if proj is not None:
+            t0 = time.perf_counter()
+            for i in range(0, self.n_total, 64):
+                self.add_projections(np.arange(i, min(i + 64, self.n_total)), proj[:, i:i + 64, :])
+            if verbose:
+                torch.cuda.synchronize(self.device)
+                print(f"[minirecast] filtered {self.n} projections ({geom.rows}x{geom.cols}) "
+                      f"in {time.perf_counter() - t0:.2f}s, backend={self.backend}")
+
+    # ----------------------------------------------------------- ingest
+    def _filter_views(self, idx, slots):
+        R, C = self.geom.rows, self.geom.cols
+        n_fft = self._tables.n_fft
+        if self.kind == "parallel":
+            return parallel_filter_views(self.geom.pixel_u, len(idx), n_fft, slots)
+        K = {k: v[idx] for k, v in self._K_all.items()}
+        return cone_filter_views(K, R, C, n_fft, slots)
+
+    def _admit(self, indices, slots, event):
+        """Make filtered slots visible to reconstructions (under the state lock)."""
+        with self._lock:
+            n0, n1 = slots[0], slots[-1] + 1
+            self._order[n0:n1] = indices
+            self._received[indices] = True
+            self._views_host[n0:n1] = self._maps_all[indices]
+            rec = self._views_host[n0:n1].view(np.uint8)
+            with torch.cuda.stream(self.ingest_stream):
+                dst = self._views_dev[n0 * N.VIEW_DTYPE.itemsize:n1 * N.VIEW_DTYPE.itemsize]
+                dst.copy_(torch.from_numpy(rec.copy()), non_blocking=False)
+            event.record(self.ingest_stream)
+            self._ingest_event = event
+            self.n = n1
+            self.version += 1
+            return self.n
+
+    def add_projections(self, indices, block):
+        """Add projections (geometry indices `indices`, data [rows, k, cols] float32)."""
+        indices = np.asarray(indices, dtype=np.int64).ravel()
+        is_tensor = isinstance(block, torch.Tensor)
+        if not is_tensor:
+            block = np.asarray(block, dtype=np.float32)
+        if block.shape[1] != len(indices):
+            raise ValueError("block has %d projections but %d indices"
+                             % (block.shape[1], len(indices)))
+        with self._ingest_lock:
+            keep = ~self._received[indices]
+            if not keep.all():
+                indices = indices[keep]
+                block = block[:, torch.from_numpy(keep)] if is_tensor else block[:, keep, :]
+            if len(indices) == 0:
+                return self.n
+            k = len(indices)
+            R, C = self.geom.rows, self.geom.cols
+            n0 = self.n
+            slots = np.arange(n0, n0 + k)
+            with torch.cuda.device(self.device), torch.cuda.stream(self.ingest_stream):
+                x = _to_device_tensor(block, self.device, torch.float32)      # [R, k, C]
+                x, s_view, s_row = preprocess.apply_device(x, self.gaussian, self.tilt)
+                fv = _struct_tensor(self._filter_views(indices, slots), self.device)
+                filter_block_device(x, s_view, s_row, k, fv, self._tables, self._ring_c,
+                                    self.ingest_stream)
+                ev = torch.cuda.Event()
+            return self._admit(indices, slots, ev)
+
+    def reset(self):
+        """Forget every received view (a new scan with the same geometry); the device
+        ring is reused."""
+        with self._ingest_lock, self._lock:
+            # new views may overwrite slots only after queued reconstructions read them
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+            self.ingest_stream.wait_event(ev)
+            self._received[:] = False
+            self.n = 0
+            self.version += 1
+
+    def set_flat_dark(self, flat, dark, bin=1, flip_rows=False, mode="flexray"):
+        """Flat / dark frames ([n, R0, C0] or [R0, C0], uint16 or float) for
+        add_raw_projections, prepared like the reference loaders: mean binning of each
+        frame, row flip (FleX-ray, flexray.py:111-116), mean over frames, then
+        gain = 1/max(F-D, 1) ("flexray", flexray.py:174-177) or 1/max(F-D, 1e-6)
+        ("hdf5", hdf5.py:64-77). Binned size must equal the geometry's rows x cols."""
+        if mode not in ("flexray", "hdf5"):
+            raise ValueError(f"unknown mode {mode!r}")
+        R, C = self.geom.rows, self.geom.cols
+        b = int(bin)
+
+        def binned(frames):
+            t = torch.as_tensor(np.asarray(frames, dtype=np.float32)).to(self.device)
+            if t.ndim == 2:
+                t = t[None]
+            h, w = t.shape[1] // b * b, t.shape[2] // b * b
+            t = t[:, :h, :w].reshape(t.shape[0], h // b, b, w // b, b).mean(dim=(2, 4))
+            if flip_rows:
+                t = torch.flip(t, dims=[1])
+            return t.mean(0)
+
+        with torch.cuda.device(self.device), torch.cuda.stream(self.ingest_stream):
+            d = binned(dark)
+            f = binned(flat)
+            if tuple(d.shape) != (R, C):
+                raise ValueError(f"binned frames are {tuple(d.shape)}, geometry is {(R, C)}")
+            eps = 1.0 if mode == "flexray" else 1e-6
+            self._dark = d.contiguous()
+            self._gain = (1.0 / torch.clamp(f - d, min=eps)).contiguous()
+        self._raw_bin, self._raw_flip = b, bool(flip_rows)
+
+    def add_raw_projections(self, indices, raw):
+        """Fused ingest of raw detector counts: raw [k, R0, C0] uint16 (NumPy, pinned or
+        CUDA tensor) -> bin, (P-D)*gain, clip 1e-3, -log, FDK weight, ramp filter, store;
+        one kernel launch (mr_ingest_u16). Needs set_flat_dark() first."""
+        if getattr(self, "_gain", None) is None:
+            raise RuntimeError("call set_flat_dark() before add_raw_projections()")
+        if self.gaussian or self.tilt:
+            raise ValueError("gaussian / tilt pre-processing needs add_projections() "
+                             "(the fused raw ingest has no neighbourhood pass)")
+        indices = np.asarray(indices, dtype=np.int64).ravel()
+        if raw.shape[0] != len(indices):
+            raise ValueError("raw has %d projections but %d indices" % (raw.shape[0], len(indices)))
+        b = self._raw_bin
+        R, C = self.geom.rows, self.geom.cols
+        if raw.shape[1] < R * b or raw.shape[2] < C * b:
+            raise ValueError(f"raw frames {tuple(raw.shape[1:])} are smaller than "
+                             f"{R * b} x {C * b}")
+        with self._ingest_lock:
+            keep = ~self._received[indices]
+            if not keep.all():
+                indices = indices[keep]
+                raw = raw[torch.from_numpy(keep)] if isinstance(raw, torch.Tensor) else raw[keep]
+            if len(indices) == 0:
+                return self.n
+            k = len(indices)
+            n0 = self.n
+            slots = np.arange(n0, n0 + k)
+            with torch.cuda.device(self.device), torch.cuda.stream(self.ingest_stream):
+                if isinstance(raw, torch.Tensor):
+                    x = raw.view(torch.int16) if raw.dtype == torch.uint16 else raw
+                    x = x.to(self.device, non_blocking=True).contiguous()
+                else:
+                    x = torch.from_numpy(np.ascontiguousarray(raw, dtype=np.uint16).view(np.int16))
+                    x = x.to(self.device, non_blocking=True)
+                if x.element_size() != 2:
+                    raise ValueError("raw counts must be 16-bit")
+                fv = _struct_tensor(self._filter_views(indices, slots), self.device)
+                lib = N.load()
+                t = self._tables
+                tm = self.kernel_timer
+                ev0 = tm.start(self.ingest_stream) if tm is not None else None
+                st = lib.mr_ingest_u16(ctypes_void(x.data_ptr()), x.shape[1] * x.shape[2], x.shape[2], b,
+                                       int(self._raw_flip), ctypes_void(self._dark.data_ptr()),
+                                       ctypes_void(self._gain.data_ptr()), k, ctypes_void(fv.data_ptr()),
+                                       ctypes_void(t.H.data_ptr()), ctypes_void(t.tw.data_ptr()), t.log2n,
+                                       self._ring_c, ctypes_void(self.ingest_stream.cuda_stream))
+                if tm is not None:
+                    tm.stop("mr_ingest_u16", ev0, self.ingest_stream)
+                N.check(st, "mr_ingest_u16")
+                x.record_stream(self.ingest_stream)
+                ev = torch.cuda.Event()
+            return self._admit(indices, slots, ev)
+
+    # ----------------------------------------------------------- info
+    @property
+    def native_pixel(self):
+        """Detector pixel size at the rotation axis (mm)."""
+        if self.kind == "parallel":
+            return float(self.geom.pixel_u)
+        K = self._K_all
+        return float(np.linalg.norm(K["u"][0]) * K["sod"][0] / K["sdd"][0])
+
+    def info(self):
+        return dict(kind=self.kind, n=int(self.n), n_total=int(self.n_total),
+                    version=int(self.version), cor_shift=float(self.cor_shift),
+                    box=[float(b) for b in self.box], native_pixel=self.native_pixel,
+                    backend=self.backend)
+
+    def plane_size(self, normal):
+        return plane_size_for_box(self.box, normal)
+
+    def inside_box(self, pts):
+        return np.all(np.abs(pts) <= self.box, axis=-1)
+
+    # ----------------------------------------------------------- reconstruction
+    def _snapshot(self):
+        with self._lock:
+            return self.n, self.cor_shift, self._ingest_event
+
+    def _run_grids(self, grids, out, n, event):
+        """Launch one batched back-projection of `grids` into device `out`."""
+        stream = self.stream
+        if event is not None:
+            stream.wait_event(event)
+        grids["n_views"] = n
+        grids["scale"] = np.pi / n if n else 0.0
+        with torch.cuda.device(self.device), torch.cuda.stream(stream):
+            backproject_device(self._ring_c, self._views_dev, grids, out, stream, self.device,
+                               self.kernel_timer)
+
+    def reconstruct_points_tensor(self, pts, cor_shift=None):
+        """Device variant of reconstruct_points: pts (M, 3) -> f32 tensor [M]."""
+        n, shift, ev = self._snapshot()
+        if cor_shift is not None:
+            shift = float(cor_shift)
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            p = _to_device_tensor(pts, self.device, torch.float32).reshape(-1, 3).contiguous()
+            M = p.shape[0]
+            out = torch.zeros(M, dtype=torch.float32, device=self.device)
+            if n == 0 or M == 0:
+                return out
+            g = np.zeros(1, dtype=N.GRID_DTYPE)
+            g["n_i"], g["n_j"], g["n_k"] = 1, M, 1
+            g["flags"] = N.MR_GRID_POINTS
+            g["out_stride_j"] = 1
+            g["points"] = p.data_ptr()
+            g["cor_shift"] = shift
+            self._run_grids(g, out, n, ev)
+            p.record_stream(self.stream)
+        return out
+
+    def reconstruct_points(self, pts, cor_shift=None):
+        pts = np.ascontiguousarray(np.asarray(pts, dtype=np.float64).reshape(-1, 3))
+        out = self.reconstruct_points_tensor(pts, cor_shift)
+        with torch.cuda.stream(self.stream):
+            return out.cpu().numpy().astype(np.float64)
+
+    def plane_grid(self, origin, normal, n=256, size=None, zoom=1.0, center=None, cor_shift=None):
+        shift = self.cor_shift if cor_shift is None else float(cor_shift)
+        return plane_grid(self.box, origin, normal, int(n), size, zoom, center, shift)
+
+    def reconstruct_planes_tensor(self, requests):
+        """Back-project many slices in ONE launch. `requests` is a list of dicts with
+        the reconstruct_plane arguments (origin, normal, n, size, zoom, center,
+        cor_shift). Returns a list of f32 device tensors [n, n]."""
+        n_views, shift, ev = self._snapshot()
+        grids = np.zeros(len(requests), dtype=N.GRID_DTYPE)
+        sizes, offset = [], 0
+        for r, req in enumerate(requests):
+            req = dict(req)
+            if req.get("cor_shift") is None:
+                req["cor_shift"] = shift
+            grids[r] = plane_grid(self.box, req["origin"], req["normal"], int(req.get("n", 256)),
+                                  req.get("size"), req.get("zoom", 1.0), req.get("center"),
+                                  float(req["cor_shift"]))
+            grids[r]["out_offset"] = offset
+            sizes.append(int(req.get("n", 256)))
+            offset += sizes[-1] ** 2
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            out = torch.zeros(offset, dtype=torch.float32, device=self.device)
+            if n_views > 0 and offset > 0:
+                self._run_grids(grids, out, n_views, ev)
+        res, o = [], 0
+        for s in sizes:
+            res.append(out[o:o + s * s].view(s, s))
+            o += s * s
+        return res
+
+    def reconstruct_planes(self, requests):
+        """Batched reconstruct_plane without the point arrays: list of f64 images."""
+        imgs = self.reconstruct_planes_tensor(requests)
+        with torch.cuda.stream(self.stream):
+            return [im.cpu().numpy().astype(np.float64) for im in imgs]
+
+    def reconstruct_plane(self, origin, normal, n=256, size=None, zoom=1.0, center=None,
+                          cor_shift=None):
+        """Reconstruct an n x n slice of the plane through `origin` with the given normal.
+        Returns (image [n, n] float64, points [n, n, 3]); pixels outside the box are 0."""
+        img = self.reconstruct_planes([dict(origin=origin, normal=normal, n=n, size=size,
+                                            zoom=zoom, center=center, cor_shift=cor_shift)])[0]
+        pts, _ = slice_points(self.box, origin, normal, n, size, zoom, center)
+        return img, pts
+
+    def _volume_frame(self, voxel, maxdim):
+        if maxdim is not None:
+            dims, origin, h = volume_grid(self.box, maxdim)
+        else:
+            h = float(voxel or self.native_pixel)
+            dims = np.maximum(np.ceil(2.0 * self.box / h).astype(int), 2)
+            origin = -self.box + h / 2.0
+        return tuple(int(d) for d in dims), np.asarray(origin, float), h
+
+    def reconstruct_volume_tensor(self, voxel=None, maxdim=None, chunk=None, progress=None,
+                                  out=None):
+        """Device variant of reconstruct_volume: returns (f32 tensor [nx, ny, nz], origin, h)."""
+        dims, origin, h = self._volume_frame(voxel, maxdim)
+        nx, ny, nz = dims
+        n_views, shift, ev = self._snapshot()
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            vol = out if out is not None else torch.empty((nx, ny, nz), dtype=torch.float32,
+                                                          device=self.device)
+            if n_views == 0:
+                vol.zero_()
+                return vol, origin, h
+            planes = nx if chunk is None else max(1, int(chunk) // (ny * nz))
+            for k0 in range(0, nx, planes):
+                k1 = min(nx, k0 + planes)
+                g = np.zeros(1, dtype=N.GRID_DTYPE)
+                g[0] = volume_grid_record(origin, h, dims, k0, k1)
+                g["cor_shift"] = shift
+                self._run_grids(g, vol.view(-1), n_views, ev)
+                if progress is not None:
+                    self.stream.synchronize()
+                    progress((k1 - 1) / max(nx - 1, 1))
+        return vol, origin, h
+
+    def reconstruct_volume(self, voxel=None, maxdim=None, chunk=262144, progress=None):
+        """Full 3D reconstruction of the volume box on a regular grid.
+        Returns (volume [nx, ny, nz] float32, origin (mm), voxel size (mm))."""
+        vol, origin, h = self.reconstruct_volume_tensor(voxel, maxdim, None, progress)
+        with torch.cuda.stream(self.stream):
+            return vol.cpu().numpy(), origin, h
+
+    def preview_volume(self, maxdim=64, chunk=65536):
+        return self.reconstruct_volume(maxdim=maxdim, chunk=chunk)
+
+    def warmup(self):
+        """Load the library and run one tiny back-projection (no JIT involved)."""
+        if self.n == 0:
+            return
+        self.reconstruct_points(np.zeros((4, 3)))
+
+    # ----------------------------------------------------------- rotation centre
+    def set_cor_shift(self, px):
+        """Take the rotation axis to project `px` detector columns right of nominal."""
+        with self._lock:
+            self.cor_shift = float(px)
+            self.version += 1
+
+    def cor_scores(self, shifts, n=192, z=0.0):
+        """-entropy of the axial slice at z for every trial shift (one batched launch)."""
+        reqs = [dict(origin=(0.0, 0.0, z), normal=(0.0, 0.0, 1.0), n=n, cor_shift=float(s))
+                for s in shifts]
+        imgs = self.reconstruct_planes(reqs)
+        scores = []
+        for img in imgs:
+            hist, _ = np.histogram(img[img != 0], bins=128)
+            prob = hist[hist > 0] / max(hist.sum(), 1)
+            scores.append(float(np.sum(prob * np.log(prob))))
+        return np.array(scores)
+
+    def estimate_cor(self, shifts=None, n=192, z=0.0, verbose=True):
+        """Pick the COR shift whose central axial slice has the lowest histogram entropy
+        (recon.py:498-519); all trial slices go in one batched launch."""
+        if shifts is None:
+            shifts = np.arange(-3.0, 3.01, 0.25)
+        shifts = np.asarray(shifts, dtype=float)
+        scores = self.cor_scores(shifts, n, z)
+        best = float(shifts[int(np.argmax(scores))])
+        self.set_cor_shift(best)
+        if verbose:
+            print("[minirecast] COR search: " + " ".join(
+                f"{s:+.2f}:{v:.3g}" for s, v in zip(shifts, scores)))
+            print(f"[minirecast] best COR shift {best:+.2f} px")
+        return best, scores
