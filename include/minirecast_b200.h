@@ -146,6 +146,15 @@ int mr_backproject(const mr_ring* ring, const mr_view* views_dev,
                    const mr_grid* grids_dev, const mr_tile* tiles_dev, int64_t n_tiles,
                    float* out_dev, void* stream);
 
+/* Same contract as mr_backproject for regular grids (not MR_GRID_POINTS), with the
+ * detector footprint of every (tile, view) staged into shared memory by the TMA unit
+ * (cp.async.bulk.tensor, zero fill outside the detector) and predicate-free software
+ * bilinear. The ring needs 16-byte aligned data, rows and slots. `status_dev` (may be
+ * NULL) receives MR_ERR_TIMEOUT if a bounded wait on a stage ever gave up. */
+int mr_backproject_staged(const mr_ring* ring, const mr_view* views_dev,
+                          const mr_grid* grids_dev, const mr_tile* tiles_dev, int64_t n_tiles,
+                          float* out_dev, int32_t* status_dev, void* stream);
+
 /* ---- filtering ---------------------------------------------------------------------
  * Replaces recon.py:85-104 (fdk_filter_block) and recon.py:58-64 (filter_rows, via
  * ramp_response 34-55) as called from add_projections recon.py:357-362.

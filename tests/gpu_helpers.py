@@ -27,11 +27,13 @@ class DeviceRing:
         self.c = R._ring_struct(self.ring, code, kind, Rr, C)
         self.stored = self.ring[:, :, :C].float().cpu().numpy() * qs[:, None, None]
 
-    def run(self, grids, n_out):
+    def run(self, grids, n_out, kernel="staged"):
         out = torch.full((n_out,), float("nan"), dtype=torch.float32, device=self.dev)
+        status = torch.zeros(1, dtype=torch.int32, device=self.dev)
         st = torch.cuda.current_stream()
-        R.backproject_device(self.c, self.views, grids, out, st, self.dev)
+        R.backproject_device(self.c, self.views, grids, out, st, self.dev, kernel=kernel, status=status)
         torch.cuda.synchronize()
+        assert int(status.item()) == 0, "device-side wait timed out"
         return out.cpu().numpy().astype(np.float64)
 
     def points(self, pts, n_views, scale, shift=0.0):

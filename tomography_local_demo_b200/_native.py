@@ -54,6 +54,7 @@ SIGNATURES = {
     "mr_bp_tile_shape": (None, [ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
     "mr_plan_tiles": (ctypes.c_int, [_P, _I32, _P, _I64, ctypes.POINTER(_I64)]),
     "mr_backproject": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P]),
+    "mr_backproject_staged": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P, _P]),
     "mr_filter_f32": (ctypes.c_int, [_P, _I64, _I64, _I32, _P, _P, _P, _I32,
                                      ctypes.POINTER(MrRing), _P]),
     "mr_ingest_u16": (ctypes.c_int, [_P, _I64, _I64, _I32, _I32, _P, _P, _I32, _P, _P, _P, _I32,

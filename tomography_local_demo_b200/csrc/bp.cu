@@ -76,8 +76,12 @@ bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_st
     __shared__ mr_grid s_g;
 
     const mr_tile t = tiles[blockIdx.x];
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int tid = ty * BP_TJ + tx;
+    const int tid = threadIdx.y * BP_TJ + threadIdx.x;
+    // Each warp covers compact 8 (j) x 4 (i) sample patches, so the detector footprint
+    // of one warp-wide gather is a small 2D patch whatever the plane orientation.
+    const int warp = tid >> 5, lane = tid & 31;
+    const int tx = ((warp & 3) << 3) | (lane & 7);            // j offset in the tile, 0..31
+    const int ty = ((warp >> 2) << 4) | (lane >> 3);          // i offset of p = 0; +4 per p
     if (tid < (int)(sizeof(mr_grid) / 4))
         reinterpret_cast<int*>(&s_g)[tid] = reinterpret_cast<const int*>(grids + t.grid)[tid];
     __syncthreads();
@@ -100,7 +104,7 @@ bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_st
         bool any = false;
 #pragma unroll
         for (int p = 0; p < BP_PPT; ++p) {
-            const int i = t.i0 + ty + BP_TY * p, j = t.j0 + tx;
+            const int i = t.i0 + ty + 4 * p, j = t.j0 + tx;
             bool ok = i < g.n_i && j < g.n_j;
             if (ok && (g.flags & MR_GRID_MASK_BOX)) ok = in_box_fp64(g, i, j);
             inside[p] = ok;
@@ -141,7 +145,7 @@ bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_st
                         const float bw = fmaf(fj, cw.z, cw.x);
 #pragma unroll
                         for (int p = 0; p < BP_PPT; ++p) {
-                            const float fi = (float)(ty + BP_TY * p);
+                            const float fi = (float)(ty + 4 * p);
                             const float nu = fmaf(fi, cu.y, bu);
                             const float nvv = fmaf(fi, cv.y, bv);
                             const float nw = fmaf(fi, cw.y, bw);
@@ -152,7 +156,7 @@ bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_st
                     } else {
 #pragma unroll
                         for (int p = 0; p < BP_PPT; ++p) {
-                            const float fi = (float)(ty + BP_TY * p);
+                            const float fi = (float)(ty + 4 * p);
                             const float val = bilerp(q, R, C, pitch, fmaf(fi, cv.y, bv), fmaf(fi, cu.y, bu));
                             acc[p] = fmaf(cu.w, val, acc[p]);
                         }
@@ -162,7 +166,7 @@ bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_st
         }
 #pragma unroll
         for (int p = 0; p < BP_PPT; ++p) {
-            const int i = t.i0 + ty + BP_TY * p, j = t.j0 + tx;
+            const int i = t.i0 + ty + 4 * p, j = t.j0 + tx;
             if (i < g.n_i && j < g.n_j) {
                 const long long o = g.out_offset + (long long)i * g.out_stride_i +
                                     (long long)j * g.out_stride_j + (long long)t.k * g.out_stride_k;

@@ -1,0 +1,461 @@
+// TMA-staged voxel-driven back-projection for regular grids (slices, windows, volumes).
+//
+// Same result as bp.cu (minirecast recon.py:156-219 semantics), different data path:
+//   * per (tile, view) the CTA projects the tile's 4 corners (a planar tile maps to the
+//     convex hull of its corners' projections) and derives the detector footprint;
+//   * one thread issues cp.async.bulk.tensor 3D box loads (W cols x 8 rows, single CTA,
+//     no multicast) of that footprint into a shared-memory stage; loads outside the
+//     detector are zero-filled by the TMA unit, which is exactly the reference's
+//     "bilinear taps outside [0,R)x[0,C) contribute 0";
+//   * a warp-specialised ring of stages: one producer warp computes footprints and issues
+//     the TMA loads, eight consumer warps back-project; full/empty mbarriers (bounded
+//     waits) are the only synchronisation inside the view loop;
+//   * the consumer loop is predicate-free: floor via a round-down FMA against a magic
+//     constant (FMA pipe only), one unsigned clamp for memory safety, four LDS, lerps;
+//   * footprints that miss the detector entirely are skipped (exactly zero), and the
+//     rare footprints larger than a stage fall back to predicated global loads.
+// Each warp covers compact 8 (j) x 4 (i) sample patches so its LDS gathers touch a small
+// 2D patch (few bank conflicts) for any plane orientation.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "mr_common.cuh"
+
+namespace mr {
+
+constexpr int ST_TI = 32, ST_TJ = 32;        // tile (samples) - same tiling as bp.cu
+constexpr int ST_CONSUMERS = 8;               // consumer warps (one 32 x 32 tile)
+constexpr int ST_THREADS = 32 * (ST_CONSUMERS + 1);   // + one producer warp
+constexpr int ST_PPT = 4;                     // samples per consumer thread (i, i+4, i+8, i+12)
+constexpr int ST_BOX_H = 8;                   // rows per TMA box
+constexpr int ST_MAX_BOXES = 10;              // <= 80 staged rows per view
+constexpr float MAGIC = 12582912.0f;          // 1.5 * 2^23
+constexpr int MAGIC_BITS = 0x4B400000;
+
+template <typename T> struct StageGeom;
+// Row widths (elements) are 16-byte multiples whose word pitch shifts successive rows
+// across banks (88 bf16 = 44 words, 84 f32 = 84 words).
+template <> struct StageGeom<__nv_bfloat16> { static constexpr int W = 88, ALIGN = 8, STAGES = 4; };
+template <> struct StageGeom<__half> { static constexpr int W = 88, ALIGN = 8, STAGES = 4; };
+template <> struct StageGeom<float> { static constexpr int W = 84, ALIGN = 4, STAGES = 3; };
+
+enum : int { MODE_STAGED = 0, MODE_GLOBAL = 1, MODE_SKIP = 2 };
+
+struct __align__(16) ViewMeta {
+    float4 cu, cv, cw;       // (value at tile origin, d/di, d/dj, qscale|-|-) in local coords
+    int x0, r0, nbox, mode;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after `limit` polls and reports it (never spins forever).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status) {
+    for (int it = 0; it < (1 << 22); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (status) atomicExch(status, MR_ERR_TIMEOUT);
+    return false;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ float lds_elem(uint32_t addr);
+template <>
+__device__ __forceinline__ float lds_elem<float>(uint32_t addr) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    return v;
+}
+template <>
+__device__ __forceinline__ float lds_elem<__nv_bfloat16>(uint32_t addr) {
+    unsigned short u;
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(u) : "r"(addr));
+    return __uint_as_float(static_cast<uint32_t>(u) << 16);
+}
+template <>
+__device__ __forceinline__ float lds_elem<__half>(uint32_t addr) {
+    unsigned short u;
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(u) : "r"(addr));
+    return __half2float(__ushort_as_half(u));
+}
+
+// Global-memory bilinear (fallback for footprints larger than a stage).
+template <typename T>
+__device__ __forceinline__ float bilerp_global(const T* __restrict__ q, int R, int C, int pitch,
+                                               float row, float col) {
+    row = fminf(fmaxf(row, -2.f), (float)R + 1.f);
+    col = fminf(fmaxf(col, -2.f), (float)C + 1.f);
+    const float r0f = floorf(row), c0f = floorf(col);
+    const float fr = row - r0f, fc = col - c0f;
+    const int r0 = (int)r0f, c0 = (int)c0f;
+    const bool rin0 = (unsigned)r0 < (unsigned)R, rin1 = (unsigned)(r0 + 1) < (unsigned)R;
+    const bool cin0 = (unsigned)c0 < (unsigned)C, cin1 = (unsigned)(c0 + 1) < (unsigned)C;
+    const T* p = q + (ptrdiff_t)r0 * pitch + c0;
+    const float q00 = (rin0 && cin0) ? ld_elem(p) : 0.f;
+    const float q01 = (rin0 && cin1) ? ld_elem(p + 1) : 0.f;
+    const float q10 = (rin1 && cin0) ? ld_elem(p + pitch) : 0.f;
+    const float q11 = (rin1 && cin1) ? ld_elem(p + pitch + 1) : 0.f;
+    const float a = fmaf(fc, q01 - q00, q00);
+    const float b = fmaf(fc, q11 - q10, q10);
+    return fmaf(fr, b - a, a);
+}
+
+__device__ __forceinline__ bool in_box_fp64_t(const mr_grid& g, int i, int j) {
+    const double aj = __dmul_rn((double)j - g.mask_half, g.mask_delta);
+    const double ai = __dmul_rn((double)i - g.mask_half, g.mask_delta);
+    bool ok = true;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const double p = __dadd_rn(__dadd_rn(g.mask_c[e], __dmul_rn(aj, g.mask_ej[e])),
+                                   __dmul_rn(ai, g.mask_ei[e]));
+        ok = ok && (fabs(p) <= g.box[e]);
+    }
+    return ok;
+}
+
+// Per-view footprint + local affine coefficients of one tile (computed by one lane of
+// the producer warp).
+template <int KIND, typename T>
+__device__ __forceinline__ ViewMeta view_meta(const mr_view& V, const mr_grid& g, float shift, float ox,
+                                              float oy, float oz, int di_max, int dj_max, int R, int C) {
+    constexpr int W = StageGeom<T>::W;
+    float pu[4], pv[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        pu[e] = fmaf(shift, V.pw[e], V.pu[e]);
+        pv[e] = fmaf(shift * V.uv, V.pw[e], V.pv[e]);
+    }
+    auto aff = [&](const float* m) {
+        return make_float3(fmaf(m[0], ox, fmaf(m[1], oy, fmaf(m[2], oz, m[3]))),
+                           fmaf(m[0], g.step_i[0], fmaf(m[1], g.step_i[1], m[2] * g.step_i[2])),
+                           fmaf(m[0], g.step_j[0], fmaf(m[1], g.step_j[1], m[2] * g.step_j[2])));
+    };
+    const float3 au = aff(pu), av = aff(pv), aw = aff(V.pw);
+    float cmin = 3e38f, cmax = -3e38f, rmin = 3e38f, rmax = -3e38f;
+    bool behind = false;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float di = (c & 1) ? (float)di_max : 0.f;
+        const float dj = (c & 2) ? (float)dj_max : 0.f;
+        const float w = fmaf(di, aw.y, fmaf(dj, aw.z, aw.x));
+        float cc = fmaf(di, au.y, fmaf(dj, au.z, au.x));
+        float rr = fmaf(di, av.y, fmaf(dj, av.z, av.x));
+        if (KIND == MR_CONE) {
+            behind |= !(w > 1e-3f);
+            const float inv = 1.f / w;
+            cc *= inv;
+            rr *= inv;
+        }
+        cmin = fminf(cmin, cc); cmax = fmaxf(cmax, cc);
+        rmin = fminf(rmin, rr); rmax = fmaxf(rmax, rr);
+    }
+    ViewMeta m;
+    int mode = MODE_GLOBAL, x0 = 0, r0 = 0, nbox = 0;
+    if (!behind && cmax == cmax && rmax == rmax && cmin == cmin && rmin == rmin) {
+        if (cmax < -2.f || cmin > (float)C + 1.f || rmax < -2.f || rmin > (float)R + 1.f) {
+            mode = MODE_SKIP;
+        } else if (cmax - cmin < (float)(W - StageGeom<T>::ALIGN - 4) &&
+                   rmax - rmin < (float)(ST_BOX_H * ST_MAX_BOXES - 4)) {
+            x0 = ((int)floorf(cmin) - 1) & ~(StageGeom<T>::ALIGN - 1);
+            r0 = (int)floorf(rmin) - 1;
+            const int rows = (int)floorf(rmax) + 3 - r0;
+            nbox = (rows + ST_BOX_H - 1) / ST_BOX_H;
+            if ((int)floorf(cmax) + 3 - x0 <= W && nbox <= ST_MAX_BOXES) mode = MODE_STAGED;
+        }
+    }
+    if (mode == MODE_STAGED) {
+        const float fx0 = (float)x0, fr0 = (float)r0;
+        m.cu = make_float4(fmaf(-fx0, aw.x, au.x), fmaf(-fx0, aw.y, au.y), fmaf(-fx0, aw.z, au.z), V.qscale);
+        m.cv = make_float4(fmaf(-fr0, aw.x, av.x), fmaf(-fr0, aw.y, av.y), fmaf(-fr0, aw.z, av.z), 0.f);
+    } else {
+        m.cu = make_float4(au.x, au.y, au.z, V.qscale);
+        m.cv = make_float4(av.x, av.y, av.z, 0.f);
+    }
+    m.cw = make_float4(aw.x, aw.y, aw.z, 0.f);
+    m.x0 = x0; m.r0 = r0; m.nbox = nbox; m.mode = mode;
+    return m;
+}
+
+// Warp-specialised: warps 0..7 consume (256 threads x 4 samples = one 32x32 tile), warp 8
+// produces. Stage s carries the TMA data and its ViewMeta; full[s] (1 arrival + TMA bytes)
+// and empty[s] (one arrival per consumer warp) hand it back and forth. No CTA-wide barrier
+// in the view loop, so consumer warps may run up to S views apart.
+template <int KIND, typename T>
+__global__ void __launch_bounds__(ST_THREADS)
+bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__ ring, int R, int C,
+                 int pitch, long long slot_stride, const mr_view* __restrict__ views,
+                 const mr_grid* __restrict__ grids, const mr_tile* __restrict__ tiles,
+                 float* __restrict__ out, int* status) {
+    constexpr int W = StageGeom<T>::W;
+    constexpr int S = StageGeom<T>::STAGES;
+    constexpr int ESZ = (int)sizeof(T);
+    constexpr int STAGE_BYTES = W * ST_BOX_H * ST_MAX_BOXES * ESZ;
+    constexpr int BOX_BYTES = W * ST_BOX_H * ESZ;
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // TMA destinations must be 128-byte aligned: round the dynamic buffer up (the host
+    // allocates 128 spare bytes), whatever static shared memory precedes it.
+    unsigned char* stages = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
+    ViewMeta* meta_ring = reinterpret_cast<ViewMeta*>(stages + S * STAGE_BYTES);   // S
+    ViewMeta* meta_new = meta_ring + S;                                              // 32
+    uint64_t* full = reinterpret_cast<uint64_t*>(meta_new + 32);                    // S
+    uint64_t* empty = full + S;                                                      // S
+    __shared__ mr_grid s_g;
+
+    const mr_tile t = tiles[blockIdx.x];
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const bool producer = warp == ST_CONSUMERS;
+    if (tid < (int)(sizeof(mr_grid) / 4))
+        reinterpret_cast<int*>(&s_g)[tid] = reinterpret_cast<const int*>(grids + t.grid)[tid];
+    if (tid < S) {
+        mbar_init(&full[tid], 1);
+        mbar_init(&empty[tid], ST_CONSUMERS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    __syncthreads();
+    const mr_grid& g = s_g;
+    const int nv = g.n_views;
+
+    const float ox = g.origin[0] + t.i0 * g.step_i[0] + t.j0 * g.step_j[0] + t.k * g.step_k[0];
+    const float oy = g.origin[1] + t.i0 * g.step_i[1] + t.j0 * g.step_j[1] + t.k * g.step_k[1];
+    const float oz = g.origin[2] + t.i0 * g.step_i[2] + t.j0 * g.step_j[2] + t.k * g.step_k[2];
+    const int tx = ((warp & 3) << 3) | (lane & 7);
+    const int ty = ((warp >> 2) << 4) | (lane >> 3);
+    bool inside[ST_PPT];
+    bool any = false;
+#pragma unroll
+    for (int p = 0; p < ST_PPT; ++p) {
+        const int i = t.i0 + ty + 4 * p, j = t.j0 + tx;
+        bool ok = !producer && i < g.n_i && j < g.n_j;
+        if (ok && (g.flags & MR_GRID_MASK_BOX)) ok = in_box_fp64_t(g, i, j);
+        inside[p] = ok;
+        any |= ok;
+    }
+    const bool tile_live = __syncthreads_or(any) != 0;
+
+    if (producer) {
+        if (!tile_live) return;
+        const int di_max = min(ST_TI, g.n_i - t.i0) - 1;
+        const int dj_max = min(ST_TJ, g.n_j - t.j0) - 1;
+        for (int vb = 0; vb < nv; vb += 32) {
+            const int cnt = min(32, nv - vb);
+            __syncwarp();
+            if (lane < cnt)
+                meta_new[lane] = view_meta<KIND, T>(views[vb + lane], g, g.cor_shift, ox, oy, oz, di_max,
+                                                    dj_max, R, C);
+            __syncwarp();
+            if (lane == 0) {
+                for (int l = 0; l < cnt; ++l) {
+                    const int v = vb + l, s = v % S, u = v / S;
+                    if (u > 0) mbar_wait(&empty[s], (u - 1) & 1, status);
+                    const ViewMeta m = meta_new[l];
+                    meta_ring[s] = m;
+                    if (m.mode == MODE_STAGED) {
+                        mbar_arrive_tx(&full[s], (uint32_t)(m.nbox * BOX_BYTES));
+                        unsigned char* dst = stages + s * STAGE_BYTES;
+                        for (int b = 0; b < m.nbox; ++b)
+                            tma_load_3d(dst + b * BOX_BYTES, &tmap, m.x0, m.r0 + b * ST_BOX_H, v, &full[s]);
+                    } else {
+                        mbar_arrive(&full[s]);
+                    }
+                }
+            }
+        }
+        return;
+    }
+
+    float acc[ST_PPT];
+#pragma unroll
+    for (int p = 0; p < ST_PPT; ++p) acc[p] = 0.f;
+    if (tile_live) {
+        const float fj = (float)tx;
+        for (int v = 0; v < nv; ++v) {
+            const int s = v % S;
+            mbar_wait(&full[s], (uint32_t)((v / S) & 1), status);
+            const ViewMeta m = meta_ring[s];
+            const float bu = fmaf(fj, m.cu.z, m.cu.x);
+            const float bv = fmaf(fj, m.cv.z, m.cv.x);
+            const float bw = fmaf(fj, m.cw.z, m.cw.x);
+            if (m.mode == MODE_STAGED) {
+                const uint32_t base = smem_u32(stages + s * STAGE_BYTES);
+                const uint32_t maxoff = (uint32_t)(m.nbox * BOX_BYTES - (W + 1) * ESZ - ESZ);
+                // byte offset = (bits_r - MAGIC_BITS) * W*ESZ + (bits_c - MAGIC_BITS) * ESZ
+                const uint32_t kofs = (uint32_t)MAGIC_BITS * (uint32_t)(W * ESZ + ESZ);
+#pragma unroll
+                for (int p = 0; p < ST_PPT; ++p) {
+                    const float fi = (float)(ty + 4 * p);
+                    const float nu = fmaf(fi, m.cu.y, bu);
+                    const float nvv = fmaf(fi, m.cv.y, bv);
+                    float r = 1.f, yc, yr, fc, fr;
+                    if (KIND == MR_CONE) {
+                        r = rcp_approx(fmaf(fi, m.cw.y, bw));
+                        yc = __fmaf_rd(nu, r, MAGIC);
+                        yr = __fmaf_rd(nvv, r, MAGIC);
+                        fc = fmaf(nu, r, MAGIC - yc);
+                        fr = fmaf(nvv, r, MAGIC - yr);
+                    } else {
+                        yc = __fadd_rd(nu, MAGIC);
+                        yr = __fadd_rd(nvv, MAGIC);
+                        fc = nu + (MAGIC - yc);
+                        fr = nvv + (MAGIC - yr);
+                    }
+                    uint32_t off = (uint32_t)__float_as_int(yr) * (uint32_t)(W * ESZ) +
+                                   (uint32_t)__float_as_int(yc) * (uint32_t)ESZ - kofs;
+                    off = min(off, maxoff);
+                    const uint32_t a = base + off;
+                    const float q00 = lds_elem<T>(a);
+                    const float q01 = lds_elem<T>(a + ESZ);
+                    const float q10 = lds_elem<T>(a + W * ESZ);
+                    const float q11 = lds_elem<T>(a + W * ESZ + ESZ);
+                    const float ta = fmaf(fc, q01 - q00, q00);
+                    const float tb = fmaf(fc, q11 - q10, q10);
+                    const float val = fmaf(fr, tb - ta, ta);
+                    acc[p] = fmaf(KIND == MR_CONE ? r * r * m.cu.w : m.cu.w, val, acc[p]);
+                }
+            } else if (m.mode == MODE_GLOBAL) {
+                const T* q = ring + (long long)v * slot_stride;
+#pragma unroll
+                for (int p = 0; p < ST_PPT; ++p) {
+                    const float fi = (float)(ty + 4 * p);
+                    const float nu = fmaf(fi, m.cu.y, bu);
+                    const float nvv = fmaf(fi, m.cv.y, bv);
+                    if (KIND == MR_CONE) {
+                        const float r = rcp_approx(fmaf(fi, m.cw.y, bw));
+                        acc[p] = fmaf(r * r * m.cu.w, bilerp_global(q, R, C, pitch, nvv * r, nu * r), acc[p]);
+                    } else {
+                        acc[p] = fmaf(m.cu.w, bilerp_global(q, R, C, pitch, nvv, nu), acc[p]);
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);      // this warp is done with stage s
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < ST_PPT; ++p) {
+        const int i = t.i0 + ty + 4 * p, j = t.j0 + tx;
+        if (i < g.n_i && j < g.n_j) {
+            const long long o = g.out_offset + (long long)i * g.out_stride_i + (long long)j * g.out_stride_j +
+                                (long long)t.k * g.out_stride_k;
+            out[o] = inside[p] ? acc[p] * g.scale : 0.f;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- host side
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+template <typename T>
+static int make_ring_map(const mr_ring* ring, CUtensorMap* map) {
+    auto fn = encode_fn();
+    if (!fn) return MR_ERR_CUDA;
+    const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : (std::is_same<T, __half>::value ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                                     : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16);
+    const cuuint64_t dims[3] = {(cuuint64_t)ring->cols, (cuuint64_t)ring->rows, (cuuint64_t)ring->n_slots};
+    const cuuint64_t strides[2] = {(cuuint64_t)ring->col_pitch * sizeof(T),
+                                   (cuuint64_t)ring->slot_stride * sizeof(T)};
+    const cuuint32_t box[3] = {(cuuint32_t)StageGeom<T>::W, (cuuint32_t)ST_BOX_H, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, dt, 3, ring->data, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? MR_OK : MR_ERR_INVALID;
+}
+
+template <int KIND, typename T>
+static int launch_staged(const mr_ring* ring, const mr_view* views, const mr_grid* grids,
+                         const mr_tile* tiles, int64_t n_tiles, float* out, int* status, cudaStream_t st) {
+    CUtensorMap map;
+    int rc = make_ring_map<T>(ring, &map);
+    if (rc != MR_OK) return rc;
+    constexpr int S = StageGeom<T>::STAGES;
+    const size_t smem = (size_t)S * StageGeom<T>::W * ST_BOX_H * ST_MAX_BOXES * sizeof(T) +
+                        (S + 32) * sizeof(ViewMeta) + 2 * S * sizeof(uint64_t) + 128;
+    auto kern = bp_staged_kernel<KIND, T>;
+    MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t max_chunk = 2147483647LL;
+    for (int64_t t0 = 0; t0 < n_tiles; t0 += max_chunk) {
+        const int64_t n = (n_tiles - t0) < max_chunk ? (n_tiles - t0) : max_chunk;
+        kern<<<(unsigned)n, ST_THREADS, smem, st>>>(map, static_cast<const T*>(ring->data), ring->rows,
+                                                    ring->cols, ring->col_pitch, (long long)ring->slot_stride,
+                                                    views, grids, tiles + t0, out, status);
+    }
+    MR_CUDA_TRY(cudaGetLastError());
+    return MR_OK;
+}
+
+}  // namespace mr
+
+extern "C" int mr_backproject_staged(const mr_ring* ring, const mr_view* views, const mr_grid* grids,
+                                     const mr_tile* tiles, int64_t n_tiles, float* out, int32_t* status,
+                                     void* stream) {
+    if (!ring || !ring->data || !views || !grids || !out || n_tiles < 0) return MR_ERR_INVALID;
+    if (n_tiles > 0 && !tiles) return MR_ERR_INVALID;
+    if (ring->rows <= 0 || ring->cols <= 0 || ring->col_pitch < ring->cols || ring->n_slots <= 0)
+        return MR_ERR_INVALID;
+    if (ring->slot_stride < (int64_t)ring->rows * ring->col_pitch) return MR_ERR_INVALID;
+    if (ring->kind != MR_CONE && ring->kind != MR_PARALLEL) return MR_ERR_INVALID;
+    if ((reinterpret_cast<uintptr_t>(ring->data) & 15) != 0) return MR_ERR_INVALID;
+    if (n_tiles == 0) return MR_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool cone = ring->kind == MR_CONE;
+    switch (ring->dtype) {
+        case MR_F32:
+            if ((ring->col_pitch * 4) % 16 || (ring->slot_stride * 4) % 16) return MR_ERR_INVALID;
+            return cone ? mr::launch_staged<MR_CONE, float>(ring, views, grids, tiles, n_tiles, out, status, st)
+                        : mr::launch_staged<MR_PARALLEL, float>(ring, views, grids, tiles, n_tiles, out, status, st);
+        case MR_BF16:
+            if ((ring->col_pitch * 2) % 16 || (ring->slot_stride * 2) % 16) return MR_ERR_INVALID;
+            return cone ? mr::launch_staged<MR_CONE, __nv_bfloat16>(ring, views, grids, tiles, n_tiles, out, status, st)
+                        : mr::launch_staged<MR_PARALLEL, __nv_bfloat16>(ring, views, grids, tiles, n_tiles, out, status, st);
+        case MR_F16:
+            if ((ring->col_pitch * 2) % 16 || (ring->slot_stride * 2) % 16) return MR_ERR_INVALID;
+            return cone ? mr::launch_staged<MR_CONE, __half>(ring, views, grids, tiles, n_tiles, out, status, st)
+                        : mr::launch_staged<MR_PARALLEL, __half>(ring, views, grids, tiles, n_tiles, out, status, st);
+        default:
+            return MR_ERR_INVALID;
+    }
+}

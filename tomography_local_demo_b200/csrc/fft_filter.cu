@@ -1,0 +1,370 @@
+// Ingest + FDK/FBP row filter with register-resident FFTs (N = 32 ... 8192).
+//
+// Same contract as filter.cu (minirecast recon.py:34-104, flexray.py / hdf5.py raw
+// correction); the FFT is organised for the SM instead of pass-by-pass in shared memory:
+//   * one FFT (two detector rows packed as z = x1 + i x2; H is real and even, so the
+//     filtered rows come back as Re and Im) is owned by G = N/32 threads, each holding
+//     32 complex values in registers;
+//   * N = 32 x R2 [x R3] mixed-radix Stockham: every pass is a radix-32 / R2 / R3 DFT
+//     entirely in registers (compile-time twiddles), passes exchange through a padded
+//     shared buffer (one float2 of padding per 32 keeps the transposes bank-conflict
+//     free), synchronised per warp when G <= 32;
+//   * the first pass reads its inputs straight from global memory (correction, -log and
+//     FDK weight applied on the fly; the upper half of the zero-padded row is known to be
+//     zero and its butterflies are pruned), and the last pass of the inverse transform
+//     writes straight to the ring;
+//   * the forward transform leaves X[n] in the registers of thread n mod G, which is
+//     exactly the input layout of the inverse (forward FFT of conj(H X)), so the spectrum
+//     never goes back to shared memory.
+#include "mr_common.cuh"
+
+namespace mr {
+namespace fft {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// Taylor series (|x| <= pi after reduction), evaluated at compile time for twiddles.
+constexpr double csin_red(double x) {
+    double term = x, sum = x;
+    for (int n = 1; n < 24; ++n) {
+        term *= -x * x / ((2.0 * n) * (2.0 * n + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+constexpr double ccos_red(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int n = 1; n < 24; ++n) {
+        term *= -x * x / ((2.0 * n - 1.0) * (2.0 * n));
+        sum += term;
+    }
+    return sum;
+}
+constexpr double reduce(double x) {  // to (-pi, pi]
+    while (x > kPi) x -= 2.0 * kPi;
+    while (x <= -kPi) x += 2.0 * kPi;
+    return x;
+}
+
+// W_R^k = exp(-2 pi i k / R) for k < R/2.
+template <int R>
+struct Twiddles {
+    float re[R / 2 > 0 ? R / 2 : 1];
+    float im[R / 2 > 0 ? R / 2 : 1];
+    constexpr Twiddles() : re(), im() {
+        for (int k = 0; k < R / 2; ++k) {
+            const double a = reduce(-2.0 * kPi * k / R);
+            re[k] = (float)ccos_red(a);
+            im[k] = (float)csin_red(a);
+        }
+    }
+};
+template <int R>
+__device__ constexpr Twiddles<R> kTw{};
+
+template <int R, int K>
+__device__ __forceinline__ float2 twiddle(float2 x) {
+    if constexpr (K == 0) {
+        return x;
+    } else if constexpr (4 * K == R) {          // W = -i
+        return make_float2(x.y, -x.x);
+    } else {
+        constexpr float c = kTw<R>.re[K], s = kTw<R>.im[K];
+        return make_float2(fmaf(x.x, c, -x.y * s), fmaf(x.x, s, x.y * c));
+    }
+}
+
+// Radix-2 decimation-in-frequency DFT of R values v[OFF + S*m], m < R, in place; the
+// result X[q] sits at v[OFF + S*bitrev(q)]. ZH: the upper half of the input is zero.
+template <int R, int OFF, int S, bool ZH, int K = 0>
+__device__ __forceinline__ void dif_stage(float2* v) {
+    if constexpr (K < R / 2) {
+        const float2 a = v[OFF + S * K];
+        if constexpr (ZH) {
+            v[OFF + S * (K + R / 2)] = twiddle<R, K>(a);
+        } else {
+            const float2 b = v[OFF + S * (K + R / 2)];
+            v[OFF + S * K] = cadd(a, b);
+            v[OFF + S * (K + R / 2)] = twiddle<R, K>(csub(a, b));
+        }
+        dif_stage<R, OFF, S, ZH, K + 1>(v);
+    }
+}
+template <int R, int OFF, int S, bool ZH = false>
+__device__ __forceinline__ void dif(float2* v) {
+    if constexpr (R > 1) {
+        dif_stage<R, OFF, S, ZH>(v);
+        dif<R / 2, OFF, S>(v);
+        dif<R / 2, OFF + S * (R / 2), S>(v);
+    }
+}
+
+__host__ __device__ constexpr int bitrev(int x, int bits) {
+    int r = 0;
+    for (int b = 0; b < bits; ++b) r |= ((x >> b) & 1) << (bits - 1 - b);
+    return r;
+}
+__host__ __device__ constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x / 2); }
+__device__ __forceinline__ int pad(int a) { return a + (a >> 5); }
+
+template <int LOG2N>
+struct Plan {
+    static constexpr int N = 1 << LOG2N;
+    static constexpr int G = N / 32;                                   // threads per FFT
+    static constexpr int R2 = N >= 1024 ? 32 : N / 32;                 // 1 -> single pass
+    static constexpr int R3 = N / (32 * R2);                           // 1 -> no third pass
+    static constexpr int FPB = 256 / G;                                // FFTs per block
+    static constexpr int BUF = N + N / 32;                             // padded float2 per FFT
+};
+
+template <int G>
+__device__ __forceinline__ void fft_sync() {
+    if constexpr (G <= 32) __syncwarp(); else __syncthreads();
+}
+
+// Forward FFT of the 32 values v[r] = x[j + G r] of the thread's FFT; on return
+// v[idx] = X[j + G idx]. ZH: x[n] = 0 for n >= N/2.
+template <int LOG2N, bool ZH>
+__device__ __forceinline__ void fft32xN(float2 (&v)[32], float2* buf, const float2* __restrict__ T,
+                                        const float2* __restrict__ twN, int j) {
+    using P = Plan<LOG2N>;
+    constexpr int N = P::N, G = P::G, R2 = P::R2, R3 = P::R3;
+    // ---- pass 1: radix 32 (Ns = 1)
+    dif<32, 0, 1, ZH>(v);
+    if constexpr (R2 == 1) {               // N == 32: done, undo the bit reversal
+        float2 t[32];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) t[q] = v[bitrev(q, 5)];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) v[q] = t[q];
+        return;
+    } else {
+        fft_sync<G>();                      // previous readers of buf are done
+#pragma unroll
+        for (int q = 0; q < 32; ++q) buf[pad(32 * j + q)] = v[bitrev(q, 5)];
+        fft_sync<G>();
+        // ---- pass 2: radix R2 (Ns = 32), 32/R2 butterflies per thread
+        constexpr int NB2 = 32 / R2;
+        constexpr int L2 = ilog2(R2);
+#pragma unroll
+        for (int b = 0; b < NB2; ++b) {
+            const int jj = j + G * b;
+            const int k = jj & 31;
+#pragma unroll
+            for (int r = 0; r < R2; ++r) {
+                float2 x = buf[pad(jj + (N / R2) * r)];
+                if (r > 0) x = cmul(x, T[(r * (32 / R2)) * 32 + k]);
+                v[b * R2 + r] = x;
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < NB2; ++b) {
+            if constexpr (R2 == 32) dif<32, 0, 1>(v);
+            else dif<R2, 0, 1>(v + b * R2);
+        }
+        if constexpr (R3 == 1) {
+            // outputs X[(jj/32)*32*R2 + k + 32 m] with jj < 32 -> n = jj + 32 m = j + G (b + NB2 m)
+            float2 t[32];
+#pragma unroll
+            for (int b = 0; b < NB2; ++b)
+#pragma unroll
+                for (int m = 0; m < R2; ++m) t[b + NB2 * m] = v[b * R2 + bitrev(m, L2)];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) v[q] = t[q];
+            return;
+        } else {
+            fft_sync<G>();
+#pragma unroll
+            for (int m = 0; m < 32; ++m) {          // NB2 == 1, jj = j
+                const int k = j & 31;
+                buf[pad((j >> 5) * 1024 + k + 32 * m)] = v[bitrev(m, 5)];
+            }
+            fft_sync<G>();
+            // ---- pass 3: radix R3 (Ns = 1024), 32/R3 butterflies per thread
+            constexpr int NB3 = 32 / R3;
+            constexpr int L3 = ilog2(R3);
+#pragma unroll
+            for (int b = 0; b < NB3; ++b) {
+                const int jj = j + G * b;          // < 1024
+#pragma unroll
+                for (int r = 0; r < R3; ++r) {
+                    float2 x = buf[pad(jj + (N / R3) * r)];
+                    if (r > 0) x = cmul(x, __ldg(twN + r * jj));
+                    v[b * R3 + r] = x;
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < NB3; ++b) dif<R3, 0, 1>(v + b * R3);
+            float2 t[32];
+#pragma unroll
+            for (int b = 0; b < NB3; ++b)
+#pragma unroll
+                for (int m = 0; m < R3; ++m) t[b + NB3 * m] = v[b * R3 + bitrev(m, L3)];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) v[q] = t[q];
+        }
+    }
+}
+
+}  // namespace fft
+
+struct Filter2Args {
+    const float* block;
+    const uint16_t* raw;
+    long long s_view, s_row;
+    int bin, flip;
+    const float* dark;
+    const float* gain;
+    const mr_filter_view* views;
+    const float* H;
+    const float2* tw;            // W_N^m, m < N
+    void* ring;
+    int dtype, rows, cols, pitch;
+    long long slot_stride;
+    int k;                       // views
+};
+
+template <bool RAW>
+__device__ __forceinline__ float ingest_x(const Filter2Args& A, int v, int r, int c) {
+    if (!RAW) return __ldg(A.block + (long long)v * A.s_view + (long long)r * A.s_row + c);
+    const int b = A.bin;
+    const int rr = A.flip ? (A.rows - 1 - r) : r;
+    const uint16_t* p = A.raw + (long long)v * A.s_view + (long long)rr * b * A.s_row + (long long)c * b;
+    float s;
+    if (b == 1) {
+        s = (float)__ldg(p);
+    } else {
+        s = 0.f;
+        for (int dy = 0; dy < b; ++dy)
+            for (int dx = 0; dx < b; ++dx) s += (float)__ldg(p + (long long)dy * A.s_row + dx);
+        s = __fdiv_rn(s, (float)(b * b));
+    }
+    const int pix = r * A.cols + c;
+    const float t = (s - __ldg(A.dark + pix)) * __ldg(A.gain + pix);
+    return -__logf(fmaxf(t, 1e-3f));
+}
+
+template <int LOG2N, bool RAW>
+__global__ void __launch_bounds__(256, LOG2N >= 11 ? 1 : 2) fft_filter_kernel(Filter2Args A) {
+    using P = fft::Plan<LOG2N>;
+    constexpr int N = P::N, G = P::G, FPB = P::FPB;
+    extern __shared__ float2 sm2[];
+    float2* T = sm2;                                  // 32 x 32: T[a*32+k] = W_1024^(a k)
+    const int f = threadIdx.x / G;
+    const int j = threadIdx.x % G;
+    float2* buf = sm2 + 1024 + f * P::BUF;
+
+    if constexpr (P::R2 > 1) {
+        // W_1024^(a k) = W_N^(a k N / 1024); for N < 1024 only a multiple of 1024/N is used
+        for (int e = threadIdx.x; e < 1024; e += 256) {
+            const int a = e >> 5, k = e & 31;
+            const long long num = (long long)a * k * N;
+            T[e] = (num % 1024 == 0) ? __ldg(A.tw + (int)((num / 1024) % N)) : make_float2(0.f, 0.f);
+        }
+    }
+    __syncthreads();
+
+    const int R = A.rows, C = A.cols;
+    const int pairs = (R + 1) / 2;
+    const long long n_items = (long long)A.k * pairs;
+    for (long long base = (long long)blockIdx.x * FPB; base < n_items; base += (long long)gridDim.x * FPB) {
+        const long long item = base + f;
+        const bool live = item < n_items;              // uniform per FFT group
+        const int v = live ? (int)(item / pairs) : 0;
+        const int r1 = live ? 2 * (int)(item % pairs) : 0;
+        const mr_filter_view fv = A.views[v];
+        float2 x[32];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int c = j + G * q;
+            float a = 0.f, b = 0.f;
+            if (live && c < C) {
+                float w1 = 1.f, w2 = 1.f;
+                if (fv.sdd != 0.f) {
+                    const float aa = fmaf((float)c, fv.da, fv.a0);
+                    const float b1 = fmaf((float)r1, fv.db, fv.b0), b2 = b1 + fv.db;
+                    const float s2 = fmaf(fv.sdd, fv.sdd, aa * aa);
+                    w1 = fv.sdd * rsqrtf(fmaf(b1, b1, s2));
+                    w2 = fv.sdd * rsqrtf(fmaf(b2, b2, s2));
+                }
+                a = ingest_x<RAW>(A, v, r1, c) * w1;
+                if (r1 + 1 < R) b = ingest_x<RAW>(A, v, r1 + 1, c) * w2;
+            }
+            x[q] = make_float2(a, b);
+        }
+#pragma unroll
+        for (int q = 16; q < 32; ++q) x[q] = make_float2(0.f, 0.f);
+        fft::fft32xN<LOG2N, true>(x, buf, T, A.tw, j);
+        const float g = fv.gain * fv.out_scale;
+#pragma unroll
+        for (int q = 0; q < 32; ++q) {
+            const float h = __ldg(A.H + j + G * q) * g;
+            x[q] = make_float2(x[q].x * h, -x[q].y * h);     // conj(H X): inverse via forward FFT
+        }
+        fft::fft32xN<LOG2N, false>(x, buf, T, A.tw, j);
+        if (live) {
+            const long long o1 = (long long)fv.slot * A.slot_stride + (long long)r1 * A.pitch;
+            const bool two = r1 + 1 < R;
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                const int c = j + G * q;
+                if (c < A.pitch) {
+                    const float y1 = c < C ? x[q].x : 0.f;
+                    const float y2 = c < C ? -x[q].y : 0.f;
+                    if (A.dtype == MR_F32) {
+                        float* o = static_cast<float*>(A.ring) + o1 + c;
+                        o[0] = y1;
+                        if (two) o[A.pitch] = y2;
+                    } else if (A.dtype == MR_BF16) {
+                        __nv_bfloat16* o = static_cast<__nv_bfloat16*>(A.ring) + o1 + c;
+                        o[0] = __float2bfloat16_rn(y1);
+                        if (two) o[A.pitch] = __float2bfloat16_rn(y2);
+                    } else {
+                        __half* o = static_cast<__half*>(A.ring) + o1 + c;
+                        o[0] = __float2half_rn(y1);
+                        if (two) o[A.pitch] = __float2half_rn(y2);
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int LOG2N, bool RAW>
+static int launch_fft_filter(const Filter2Args& A, cudaStream_t st) {
+    using P = fft::Plan<LOG2N>;
+    const size_t smem = (1024 + (size_t)P::FPB * P::BUF) * sizeof(float2);
+    auto kern = fft_filter_kernel<LOG2N, RAW>;
+    MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 148;
+    MR_CUDA_TRY(cudaGetDevice(&dev));
+    MR_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long long items = (long long)A.k * ((A.rows + 1) / 2);
+    const long long need = (items + P::FPB - 1) / P::FPB;
+    const long long grid = need < 2LL * sms * 8 ? need : 2LL * sms * 8;
+    if (grid <= 0) return MR_OK;
+    kern<<<(unsigned)grid, 256, smem, st>>>(A);
+    MR_CUDA_TRY(cudaGetLastError());
+    return MR_OK;
+}
+
+template <bool RAW>
+int launch_fft_filter_any(const Filter2Args& A, int log2n, cudaStream_t st) {
+    switch (log2n) {
+        case 5: return launch_fft_filter<5, RAW>(A, st);
+        case 6: return launch_fft_filter<6, RAW>(A, st);
+        case 7: return launch_fft_filter<7, RAW>(A, st);
+        case 8: return launch_fft_filter<8, RAW>(A, st);
+        case 9: return launch_fft_filter<9, RAW>(A, st);
+        case 10: return launch_fft_filter<10, RAW>(A, st);
+        case 11: return launch_fft_filter<11, RAW>(A, st);
+        case 12: return launch_fft_filter<12, RAW>(A, st);
+        case 13: return launch_fft_filter<13, RAW>(A, st);
+        default: return MR_ERR_UNSUPPORTED;
+    }
+}
+
+template int launch_fft_filter_any<false>(const Filter2Args&, int, cudaStream_t);
+template int launch_fft_filter_any<true>(const Filter2Args&, int, cudaStream_t);
+
+}  // namespace mr

@@ -16,6 +16,24 @@
 
 namespace mr {
 
+struct Filter2Args {
+    const float* block;
+    const uint16_t* raw;
+    long long s_view, s_row;
+    int bin, flip;
+    const float* dark;
+    const float* gain;
+    const mr_filter_view* views;
+    const float* H;
+    const float2* tw;
+    void* ring;
+    int dtype, rows, cols, pitch;
+    long long slot_stride;
+    int k;
+};
+template <bool RAW>
+int launch_fft_filter_any(const Filter2Args& A, int log2n, cudaStream_t st);
+
 constexpr int FLT_THREADS = 256;
 
 struct FilterArgs {
@@ -187,6 +205,11 @@ static int launch_filter_n(const FilterArgs& A, int k, cudaStream_t st) {
 
 template <bool RAW>
 static int launch_filter(const FilterArgs& A, int log2n, int k, cudaStream_t st) {
+    if (log2n >= 5 && log2n <= 13) {            // register-resident FFT kernel
+        Filter2Args B{A.block, A.raw, A.s_view, A.s_row, A.bin, A.flip, A.dark, A.gain, A.views, A.H,
+                      A.tw, A.ring, A.dtype, A.rows, A.cols, A.pitch, A.slot_stride, k};
+        return launch_fft_filter_any<RAW>(B, log2n, st);
+    }
     switch (log2n) {
         case 4: return launch_filter_n<4, RAW>(A, k, st);
         case 5: return launch_filter_n<5, RAW>(A, k, st);
@@ -209,7 +232,6 @@ static int check_common(const mr_ring* ring, int32_t k, const mr_filter_view* vi
     if (ring->slot_stride < (int64_t)ring->rows * ring->col_pitch) return MR_ERR_INVALID;
     if (ring->dtype != MR_F32 && ring->dtype != MR_BF16 && ring->dtype != MR_F16) return MR_ERR_INVALID;
     if (log2n < 1 || log2n > 30 || (1LL << log2n) < 2LL * ring->cols) return MR_ERR_INVALID;
-    if (k > 65535) return MR_ERR_INVALID;
     return MR_OK;
 }
 

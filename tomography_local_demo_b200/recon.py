@@ -190,6 +190,19 @@ def _to_device_tensor(arr, device, dtype=None):
     return t.to(device, non_blocking=True).contiguous()
 
 
+def _handoff(stream, *tensors):
+    """Order the caller's current stream after `stream` (where `tensors` were produced)
+    and tell the allocator the tensors are used there, so results returned by the
+    *_tensor methods are safe to use on the caller's stream."""
+    cur = torch.cuda.current_stream(stream.device)
+    if cur.cuda_stream != stream.cuda_stream:
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        cur.wait_event(ev)
+        for t in tensors:
+            t.record_stream(cur)
+
+
 def _struct_tensor(records, device):
     raw = np.ascontiguousarray(records).view(np.uint8)
     return torch.from_numpy(raw.copy()).to(device, non_blocking=False)
@@ -234,21 +247,40 @@ class KernelTimer:
         self.records = []
 
 
-def backproject_device(ring, views_dev, grids, out, stream, device, timer=None):
-    """Back-project numpy GRID_DTYPE records into the device f32 tensor `out`."""
+def backproject_device(ring, views_dev, grids, out, stream, device, timer=None, kernel="staged",
+                       status=None):
+    """Back-project numpy GRID_DTYPE records into the device f32 tensor `out`.
+
+    kernel="staged": regular grids go through mr_backproject_staged (TMA-staged
+    footprints); point lists always use mr_backproject. kernel="plain": everything uses
+    mr_backproject (direct global gathers) - the plain GPU path kept for comparison."""
+    grids = np.ascontiguousarray(grids, dtype=N.GRID_DTYPE)
+    is_pts = (grids["flags"] & N.MR_GRID_POINTS) != 0
+    if kernel == "staged" and is_pts.any() and not is_pts.all():
+        backproject_device(ring, views_dev, grids[is_pts], out, stream, device, timer, "plain")
+        grids = grids[~is_pts]
+        is_pts = is_pts[~is_pts]
     tiles = N.plan_tiles(grids)
     if len(tiles) == 0:
         return
     g_dev = _struct_tensor(grids, device)
     t_dev = _struct_tensor(tiles, device)
     lib = N.load()
+    v = ctypes_void
+    staged = kernel == "staged" and not is_pts.any()
+    name = "mr_backproject_staged" if staged else "mr_backproject"
     ev0 = timer.start(stream) if timer is not None else None
-    st = lib.mr_backproject(ring, ctypes_void(views_dev.data_ptr()), ctypes_void(g_dev.data_ptr()),
-                            ctypes_void(t_dev.data_ptr()), len(tiles), ctypes_void(out.data_ptr()),
-                            ctypes_void(stream.cuda_stream))
+    if staged:
+        st = lib.mr_backproject_staged(ring, v(views_dev.data_ptr()), v(g_dev.data_ptr()), v(t_dev.data_ptr()),
+                                       len(tiles), v(out.data_ptr()),
+                                       v(status.data_ptr()) if status is not None else None,
+                                       v(stream.cuda_stream))
+    else:
+        st = lib.mr_backproject(ring, v(views_dev.data_ptr()), v(g_dev.data_ptr()), v(t_dev.data_ptr()),
+                                len(tiles), v(out.data_ptr()), v(stream.cuda_stream))
     if timer is not None:
-        timer.stop("mr_backproject", ev0, stream)
-    N.check(st, "mr_backproject")
+        timer.stop(name, ev0, stream)
+    N.check(st, name)
     # keep the descriptor tensors alive until the kernel has consumed them
     g_dev.record_stream(stream)
     t_dev.record_stream(stream)
@@ -468,6 +500,9 @@ class SliceReconstructor:
         self._ring_c = _ring_struct(self._ring, self._dtype_code, self._kind_code, R, C)
         self._ingest_event = None
         self.kernel_timer = None        # a KernelTimer records launch durations when set
+        self.bp_kernel = "staged"       # "plain": direct-gather kernel for every request
+        with torch.cuda.device(self.device):
+            self._status = torch.zeros(1, dtype=torch.int32, device=self.device)
 
         if proj is not None:
             t0 = time.perf_counter()
@@ -664,7 +699,7 @@ class SliceReconstructor:
         grids["scale"] = np.pi / n if n else 0.0
         with torch.cuda.device(self.device), torch.cuda.stream(stream):
             backproject_device(self._ring_c, self._views_dev, grids, out, stream, self.device,
-                               self.kernel_timer)
+                               self.kernel_timer, self.bp_kernel, self._status)
 
     def reconstruct_points_tensor(self, pts, cor_shift=None):
         """Device variant of reconstruct_points: pts (M, 3) -> f32 tensor [M]."""
@@ -685,50 +720,60 @@ class SliceReconstructor:
             g["cor_shift"] = shift
             self._run_grids(g, out, n, ev)
             p.record_stream(self.stream)
+        _handoff(self.stream, out)
         return out
 
     def reconstruct_points(self, pts, cor_shift=None):
         pts = np.ascontiguousarray(np.asarray(pts, dtype=np.float64).reshape(-1, 3))
         out = self.reconstruct_points_tensor(pts, cor_shift)
-        with torch.cuda.stream(self.stream):
-            return out.cpu().numpy().astype(np.float64)
+        return out.cpu().numpy().astype(np.float64)
 
     def plane_grid(self, origin, normal, n=256, size=None, zoom=1.0, center=None, cor_shift=None):
         shift = self.cor_shift if cor_shift is None else float(cor_shift)
         return plane_grid(self.box, origin, normal, int(n), size, zoom, center, shift)
 
-    def reconstruct_planes_tensor(self, requests):
-        """Back-project many slices in ONE launch. `requests` is a list of dicts with
-        the reconstruct_plane arguments (origin, normal, n, size, zoom, center,
-        cor_shift). Returns a list of f32 device tensors [n, n]."""
+    def _planes(self, requests):
+        """One batched launch for many slices -> (flat f32 device tensor, sizes)."""
         n_views, shift, ev = self._snapshot()
         grids = np.zeros(len(requests), dtype=N.GRID_DTYPE)
         sizes, offset = [], 0
         for r, req in enumerate(requests):
-            req = dict(req)
-            if req.get("cor_shift") is None:
-                req["cor_shift"] = shift
-            grids[r] = plane_grid(self.box, req["origin"], req["normal"], int(req.get("n", 256)),
-                                  req.get("size"), req.get("zoom", 1.0), req.get("center"),
-                                  float(req["cor_shift"]))
+            n = int(req.get("n", 256))
+            s_ = req.get("cor_shift")
+            grids[r] = plane_grid(self.box, req["origin"], req["normal"], n, req.get("size"),
+                                  req.get("zoom", 1.0), req.get("center"),
+                                  shift if s_ is None else float(s_))
             grids[r]["out_offset"] = offset
-            sizes.append(int(req.get("n", 256)))
-            offset += sizes[-1] ** 2
+            sizes.append(n)
+            offset += n * n
         with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
             out = torch.zeros(offset, dtype=torch.float32, device=self.device)
             if n_views > 0 and offset > 0:
                 self._run_grids(grids, out, n_views, ev)
+        _handoff(self.stream, out)
+        return out, sizes
+
+    def reconstruct_planes_tensor(self, requests):
+        """Back-project many slices in ONE launch. `requests` is a list of dicts with
+        the reconstruct_plane arguments (origin, normal, n, size, zoom, center,
+        cor_shift). Returns a list of f32 device tensors [n, n] (views of one buffer)."""
+        out, sizes = self._planes(requests)
         res, o = [], 0
-        for s in sizes:
-            res.append(out[o:o + s * s].view(s, s))
-            o += s * s
+        for n in sizes:
+            res.append(out[o:o + n * n].view(n, n))
+            o += n * n
         return res
 
     def reconstruct_planes(self, requests):
-        """Batched reconstruct_plane without the point arrays: list of f64 images."""
-        imgs = self.reconstruct_planes_tensor(requests)
-        with torch.cuda.stream(self.stream):
-            return [im.cpu().numpy().astype(np.float64) for im in imgs]
+        """Batched reconstruct_plane without the point arrays: list of f64 images
+        (one device->host copy for the whole batch)."""
+        out, sizes = self._planes(requests)
+        host = out.cpu().numpy().astype(np.float64)
+        res, o = [], 0
+        for n in sizes:
+            res.append(host[o:o + n * n].reshape(n, n))
+            o += n * n
+        return res
 
     def reconstruct_plane(self, origin, normal, n=256, size=None, zoom=1.0, center=None,
                           cor_shift=None):
@@ -770,17 +815,25 @@ class SliceReconstructor:
                 if progress is not None:
                     self.stream.synchronize()
                     progress((k1 - 1) / max(nx - 1, 1))
+        _handoff(self.stream, vol)
         return vol, origin, h
 
     def reconstruct_volume(self, voxel=None, maxdim=None, chunk=262144, progress=None):
         """Full 3D reconstruction of the volume box on a regular grid.
         Returns (volume [nx, ny, nz] float32, origin (mm), voxel size (mm))."""
         vol, origin, h = self.reconstruct_volume_tensor(voxel, maxdim, None, progress)
-        with torch.cuda.stream(self.stream):
-            return vol.cpu().numpy(), origin, h
+        return vol.cpu().numpy(), origin, h
 
     def preview_volume(self, maxdim=64, chunk=65536):
         return self.reconstruct_volume(maxdim=maxdim, chunk=chunk)
+
+    def device_status(self):
+        """Raise TimeoutError if a bounded device-side wait ever gave up (reads one
+        int32 after synchronising the reconstruction stream)."""
+        self.stream.synchronize()
+        code = int(self._status.item())
+        if code != 0:
+            N.check(code, "device-side status")
 
     def warmup(self):
         """Load the library and run one tiny back-projection (no JIT involved)."""
