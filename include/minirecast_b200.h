@@ -181,6 +181,15 @@ int mr_ingest_u16(const uint16_t* raw, int64_t s_view, int64_t s_row,
                   const float* H_dev, const float* twiddle_dev, int32_t log2n,
                   const mr_ring* ring, void* stream);
 
+/* ---- rotation-centre search score ---------------------------------------------
+ * Replaces the scoring loop of recon.py:498-519 (estimate_cor): for each of n_imgs
+ * images (f32, device, image i at imgs + i*stride, n_pix pixels) the FP64 score
+ * sum(p log p) of a `bins`-bin histogram of its non-zero pixels, with numpy.histogram's
+ * bin assignment (range = [min, max] of the non-zero pixels, top edge inclusive).
+ * scores: device, n_imgs doubles. bins <= 1024. */
+int mr_slice_entropy(const float* imgs, int32_t n_imgs, int64_t stride, int32_t n_pix,
+                     int32_t bins, double* scores_dev, void* stream);
+
 /* ---- pre-processing on arrival (block layout [rows, k, cols], f32, device) ------
  * Replaces preprocess.py:31-56 (rotate_projections): every projection rotated by
  * `degrees` about the detector centre, bilinear, zero outside. in != out. */

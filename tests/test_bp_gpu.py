@@ -191,7 +191,7 @@ def test_staged_kernel_edge_footprints(cuda, store):
     grids["n_views"], grids["scale"] = A, np.pi / A
     staged = ring.run(grids, off, "staged")
     plain = ring.run(grids, off, "plain")
-    assert rel_l2(staged, plain) < 1e-6
+    assert rel_l2(staged, plain) < 5e-5
     off = 0
     stack = ring.stored.astype(np.float32)
     for o, nrm, n, zm in cases:

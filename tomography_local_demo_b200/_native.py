@@ -59,6 +59,7 @@ SIGNATURES = {
                                      ctypes.POINTER(MrRing), _P]),
     "mr_ingest_u16": (ctypes.c_int, [_P, _I64, _I64, _I32, _I32, _P, _P, _I32, _P, _P, _P, _I32,
                                      ctypes.POINTER(MrRing), _P]),
+    "mr_slice_entropy": (ctypes.c_int, [_P, _I32, _I64, _I32, _I32, _P, _P]),
     "mr_rotate_f32": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, ctypes.c_double, _P]),
     "mr_gaussian_axis_f32": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _I32, _I32, _P, _I32, _P]),
 }

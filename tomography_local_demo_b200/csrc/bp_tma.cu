@@ -19,9 +19,12 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cooperative_groups.h>
 #include <mutex>
 
 #include "mr_common.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace mr {
 
@@ -31,6 +34,7 @@ constexpr int ST_THREADS = 32 * (ST_CONSUMERS + 1);   // + one producer warp
 constexpr int ST_PPT = 4;                     // samples per consumer thread (i, i+4, i+8, i+12)
 constexpr int ST_BOX_H = 8;                   // rows per TMA box
 constexpr int ST_MAX_BOXES = 10;              // <= 80 staged rows per view
+constexpr int ST_CLUSTER = 4;                 // CTAs per tile, each a quarter of the views
 constexpr float MAGIC = 12582912.0f;          // 1.5 * 2^23
 constexpr int MAGIC_BITS = 0x4B400000;
 
@@ -159,7 +163,14 @@ __device__ __forceinline__ ViewMeta view_meta(const mr_view& V, const mr_grid& g
                            fmaf(m[0], g.step_i[0], fmaf(m[1], g.step_i[1], m[2] * g.step_i[2])),
                            fmaf(m[0], g.step_j[0], fmaf(m[1], g.step_j[1], m[2] * g.step_j[2])));
     };
-    const float3 au = aff(pu), av = aff(pv), aw = aff(V.pw);
+    float3 au = aff(pu), av = aff(pv), aw = aff(V.pw);
+    if (KIND == MR_CONE && V.qscale != 1.f) {
+        // col = nu/nw and row = nv/nw are scale free, 1/nw^2 picks up qscale
+        const float k = rsqrtf(V.qscale);
+        au = make_float3(au.x * k, au.y * k, au.z * k);
+        av = make_float3(av.x * k, av.y * k, av.z * k);
+        aw = make_float3(aw.x * k, aw.y * k, aw.z * k);
+    }
     float cmin = 3e38f, cmax = -3e38f, rmin = 3e38f, rmax = -3e38f;
     bool behind = false;
 #pragma unroll
@@ -209,6 +220,9 @@ __device__ __forceinline__ ViewMeta view_meta(const mr_view& V, const mr_grid& g
 // produces. Stage s carries the TMA data and its ViewMeta; full[s] (1 arrival + TMA bytes)
 // and empty[s] (one arrival per consumer warp) hand it back and forth. No CTA-wide barrier
 // in the view loop, so consumer warps may run up to S views apart.
+// A thread-block cluster of ST_CLUSTER CTAs shares one tile: CTA rank r back-projects the
+// r-th quarter of the views and rank 0 sums the partials from the others' shared memory
+// (DSMEM) in rank order - deterministic, no atomics, no scratch - and writes the tile.
 template <int KIND, typename T>
 __global__ void __launch_bounds__(ST_THREADS)
 bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__ ring, int R, int C,
@@ -230,9 +244,13 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
     ViewMeta* meta_new = meta_ring + S;                                              // 32
     uint64_t* full = reinterpret_cast<uint64_t*>(meta_new + 32);                    // S
     uint64_t* empty = full + S;                                                      // S
+    float4* partial = reinterpret_cast<float4*>(empty + S);                          // 256 (cluster sum)
     __shared__ mr_grid s_g;
 
-    const mr_tile t = tiles[blockIdx.x];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank();
+    const int csize = (int)cluster.num_blocks();
+    const mr_tile t = tiles[blockIdx.x / csize];
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const bool producer = warp == ST_CONSUMERS;
@@ -245,7 +263,10 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     __syncthreads();
     const mr_grid& g = s_g;
-    const int nv = g.n_views;
+    // this CTA's share of the views: [v_begin, v_end)
+    const int v_begin = (int)(((long long)g.n_views * crank) / csize);
+    const int v_end = (int)(((long long)g.n_views * (crank + 1)) / csize);
+    const int nv = v_end - v_begin;
 
     const float ox = g.origin[0] + t.i0 * g.step_i[0] + t.j0 * g.step_j[0] + t.k * g.step_k[0];
     const float oy = g.origin[1] + t.i0 * g.step_i[1] + t.j0 * g.step_j[1] + t.k * g.step_k[1];
@@ -264,16 +285,15 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
     }
     const bool tile_live = __syncthreads_or(any) != 0;
 
-    if (producer) {
-        if (!tile_live) return;
+    if (producer && tile_live) {
         const int di_max = min(ST_TI, g.n_i - t.i0) - 1;
         const int dj_max = min(ST_TJ, g.n_j - t.j0) - 1;
         for (int vb = 0; vb < nv; vb += 32) {
             const int cnt = min(32, nv - vb);
             __syncwarp();
             if (lane < cnt)
-                meta_new[lane] = view_meta<KIND, T>(views[vb + lane], g, g.cor_shift, ox, oy, oz, di_max,
-                                                    dj_max, R, C);
+                meta_new[lane] = view_meta<KIND, T>(views[v_begin + vb + lane], g, g.cor_shift, ox, oy, oz,
+                                                    di_max, dj_max, R, C);
             __syncwarp();
             if (lane == 0) {
                 for (int l = 0; l < cnt; ++l) {
@@ -285,20 +305,20 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                         mbar_arrive_tx(&full[s], (uint32_t)(m.nbox * BOX_BYTES));
                         unsigned char* dst = stages + s * STAGE_BYTES;
                         for (int b = 0; b < m.nbox; ++b)
-                            tma_load_3d(dst + b * BOX_BYTES, &tmap, m.x0, m.r0 + b * ST_BOX_H, v, &full[s]);
+                            tma_load_3d(dst + b * BOX_BYTES, &tmap, m.x0, m.r0 + b * ST_BOX_H, v_begin + v,
+                                        &full[s]);
                     } else {
                         mbar_arrive(&full[s]);
                     }
                 }
             }
         }
-        return;
     }
 
     float acc[ST_PPT];
 #pragma unroll
     for (int p = 0; p < ST_PPT; ++p) acc[p] = 0.f;
-    if (tile_live) {
+    if (!producer && tile_live) {
         const float fj = (float)tx;
         for (int v = 0; v < nv; ++v) {
             const int s = v % S;
@@ -341,10 +361,10 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                     const float ta = fmaf(fc, q01 - q00, q00);
                     const float tb = fmaf(fc, q11 - q10, q10);
                     const float val = fmaf(fr, tb - ta, ta);
-                    acc[p] = fmaf(KIND == MR_CONE ? r * r * m.cu.w : m.cu.w, val, acc[p]);
+                    acc[p] = fmaf(KIND == MR_CONE ? r * r : m.cu.w, val, acc[p]);
                 }
             } else if (m.mode == MODE_GLOBAL) {
-                const T* q = ring + (long long)v * slot_stride;
+                const T* q = ring + (long long)(v_begin + v) * slot_stride;
 #pragma unroll
                 for (int p = 0; p < ST_PPT; ++p) {
                     const float fi = (float)(ty + 4 * p);
@@ -352,7 +372,7 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                     const float nvv = fmaf(fi, m.cv.y, bv);
                     if (KIND == MR_CONE) {
                         const float r = rcp_approx(fmaf(fi, m.cw.y, bw));
-                        acc[p] = fmaf(r * r * m.cu.w, bilerp_global(q, R, C, pitch, nvv * r, nu * r), acc[p]);
+                        acc[p] = fmaf(r * r, bilerp_global(q, R, C, pitch, nvv * r, nu * r), acc[p]);
                     } else {
                         acc[p] = fmaf(m.cu.w, bilerp_global(q, R, C, pitch, nvv, nu), acc[p]);
                     }
@@ -362,15 +382,29 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
             if (lane == 0) mbar_arrive(&empty[s]);      // this warp is done with stage s
         }
     }
-#pragma unroll
-    for (int p = 0; p < ST_PPT; ++p) {
-        const int i = t.i0 + ty + 4 * p, j = t.j0 + tx;
-        if (i < g.n_i && j < g.n_j) {
-            const long long o = g.out_offset + (long long)i * g.out_stride_i + (long long)j * g.out_stride_j +
-                                (long long)t.k * g.out_stride_k;
-            out[o] = inside[p] ? acc[p] * g.scale : 0.f;
+    // ---- cluster reduction of the view-quarter partial sums (rank order), rank 0 writes
+    if (csize > 1) {
+        if (!producer) partial[tid] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        cluster.sync();
+        if (crank == 0 && !producer) {
+            for (int r = 1; r < csize; ++r) {
+                const float4 o = cluster.map_shared_rank(partial, r)[tid];
+                acc[0] += o.x; acc[1] += o.y; acc[2] += o.z; acc[3] += o.w;
+            }
         }
     }
+    if (crank == 0 && !producer) {
+#pragma unroll
+        for (int p = 0; p < ST_PPT; ++p) {
+            const int i = t.i0 + ty + 4 * p, j = t.j0 + tx;
+            if (i < g.n_i && j < g.n_j) {
+                const long long o = g.out_offset + (long long)i * g.out_stride_i +
+                                    (long long)j * g.out_stride_j + (long long)t.k * g.out_stride_k;
+                out[o] = inside[p] ? acc[p] * g.scale : 0.f;
+            }
+        }
+    }
+    if (csize > 1) cluster.sync();          // keep every partial alive until rank 0 has read it
 }
 
 // ---------------------------------------------------------------- host side
@@ -413,15 +447,28 @@ static int launch_staged(const mr_ring* ring, const mr_view* views, const mr_gri
     if (rc != MR_OK) return rc;
     constexpr int S = StageGeom<T>::STAGES;
     const size_t smem = (size_t)S * StageGeom<T>::W * ST_BOX_H * ST_MAX_BOXES * sizeof(T) +
-                        (S + 32) * sizeof(ViewMeta) + 2 * S * sizeof(uint64_t) + 128;
+                        (S + 32) * sizeof(ViewMeta) + 2 * S * sizeof(uint64_t) +
+                        ST_CONSUMERS * 32 * sizeof(float4) + 128;
     auto kern = bp_staged_kernel<KIND, T>;
     MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int64_t max_chunk = 2147483647LL;
+    const int64_t max_chunk = 2147483647LL / ST_CLUSTER;
     for (int64_t t0 = 0; t0 < n_tiles; t0 += max_chunk) {
         const int64_t n = (n_tiles - t0) < max_chunk ? (n_tiles - t0) : max_chunk;
-        kern<<<(unsigned)n, ST_THREADS, smem, st>>>(map, static_cast<const T*>(ring->data), ring->rows,
-                                                    ring->cols, ring->col_pitch, (long long)ring->slot_stride,
-                                                    views, grids, tiles + t0, out, status);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(n * ST_CLUSTER));
+        cfg.blockDim = dim3(ST_THREADS);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = ST_CLUSTER;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        MR_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, map, static_cast<const T*>(ring->data), ring->rows,
+                                       ring->cols, ring->col_pitch, (long long)ring->slot_stride, views, grids,
+                                       tiles + t0, out, status));
     }
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;

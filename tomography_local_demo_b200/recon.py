@@ -848,17 +848,21 @@ class SliceReconstructor:
             self.cor_shift = float(px)
             self.version += 1
 
-    def cor_scores(self, shifts, n=192, z=0.0):
-        """-entropy of the axial slice at z for every trial shift (one batched launch)."""
+    def cor_scores(self, shifts, n=192, z=0.0, bins=128):
+        """-entropy of the axial slice at z for every trial shift: one batched
+        back-projection of all trial slices, then one scoring launch (mr_slice_entropy)."""
         reqs = [dict(origin=(0.0, 0.0, z), normal=(0.0, 0.0, 1.0), n=n, cor_shift=float(s))
                 for s in shifts]
-        imgs = self.reconstruct_planes(reqs)
-        scores = []
-        for img in imgs:
-            hist, _ = np.histogram(img[img != 0], bins=128)
-            prob = hist[hist > 0] / max(hist.sum(), 1)
-            scores.append(float(np.sum(prob * np.log(prob))))
-        return np.array(scores)
+        if not reqs:
+            return np.zeros(0)
+        out, _ = self._planes(reqs)
+        with torch.cuda.device(self.device):
+            st = torch.cuda.current_stream(self.device)
+            scores = torch.empty(len(reqs), dtype=torch.float64, device=self.device)
+            N.check(N.load().mr_slice_entropy(ctypes_void(out.data_ptr()), len(reqs), n * n, n * n, bins,
+                                              ctypes_void(scores.data_ptr()), ctypes_void(st.cuda_stream)),
+                    "mr_slice_entropy")
+            return scores.cpu().numpy()
 
     def estimate_cor(self, shifts=None, n=192, z=0.0, verbose=True):
         """Pick the COR shift whose central axial slice has the lowest histogram entropy
