@@ -75,7 +75,8 @@ typedef struct mr_view {
  *   c + a_j*e_j + a_i*e_i,  a_x = (x - mask_half) * mask_delta
  * lies in the box (|p_x| <= box_x for every axis), evaluated in the rounding order
  * of minirecast slice_points (recon.py:238-265), so the mask matches it bit for bit.
- * With MR_GRID_POINTS the positions are points[j*3 + 0..2] (n_i = n_k = 1). */
+ * With MR_GRID_POINTS the positions are points[j*3 + 0..2] (n_i = n_k = 1).
+ * cor_shift and the tilt act on every view's projective map (see tilt_cos below). */
 #define MR_GRID_MASK_BOX 1
 #define MR_GRID_POINTS   2
 typedef struct mr_grid {
@@ -88,11 +89,14 @@ typedef struct mr_grid {
     int32_t n_i, n_j, n_k;
     int32_t n_views;        /* use slots [0, n_views) - the snapshot at admission */
     int32_t flags;
-    int32_t pad0;
+    float   tilt;           /* detector in-plane rotation (rad), informational */
     int64_t out_offset;
     int64_t out_stride_i, out_stride_j, out_stride_k;
     const float* points;    /* device, MR_GRID_POINTS only */
-    int64_t pad1;
+    float   tilt_cos, tilt_sin;   /* (0, 0) = no tilt. Detector coordinates are rotated
+                                     about the detector centre (cc, cr) = ((C-1)/2, (R-1)/2):
+                                     col' = cc + c (col-cc) + s (row-cr) + shift,
+                                     row' = cr - s (col-cc) + c (row-cr) + shift * uv */
     double  mask_c[3];      /* plane centre */
     double  mask_ej[3];     /* unit vector along j (columns) */
     double  mask_ei[3];     /* unit vector along i (rows) */
@@ -154,6 +158,22 @@ int mr_backproject(const mr_ring* ring, const mr_view* views_dev,
 int mr_backproject_staged(const mr_ring* ring, const mr_view* views_dev,
                           const mr_grid* grids_dev, const mr_tile* tiles_dev, int64_t n_tiles,
                           float* out_dev, int32_t* status_dev, void* stream);
+
+/* ---- derivatives of the back-projection (no counterpart in minirecast: the reference
+ * back-projector is not differentiable; the forward operator is recon.py:156-219) ----
+ * Matched forward projector, the exact transpose of mr_backproject: grad_ring (F32, the
+ * ring layout, zeroed by the caller) += B^T grad_out, where grad_out has the layout of
+ * the forward output. Samples masked out of the box carry no gradient. */
+int mr_project_adjoint(const mr_ring* grad_ring, const mr_view* views_dev,
+                       const mr_grid* grids_dev, const mr_tile* tiles_dev, int64_t n_tiles,
+                       const float* grad_out_dev, void* stream);
+
+/* dgeom[2*g + 0] += d<grad_out, f_g>/d cor_shift, dgeom[2*g + 1] += d<...>/d tilt (per
+ * radian) for every grid g, with f the forward output of mr_backproject on `ring`.
+ * dgeom: device doubles, zeroed by the caller. */
+int mr_bp_grad_geom(const mr_ring* ring, const mr_view* views_dev, const mr_grid* grids_dev,
+                    const mr_tile* tiles_dev, int64_t n_tiles, const float* grad_out_dev,
+                    double* dgeom_dev, void* stream);
 
 /* ---- filtering ---------------------------------------------------------------------
  * Replaces recon.py:85-104 (fdk_filter_block) and recon.py:58-64 (filter_rows, via

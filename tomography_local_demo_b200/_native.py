@@ -27,9 +27,9 @@ VIEW_DTYPE = np.dtype([("pu", "<f4", 4), ("pv", "<f4", 4), ("pw", "<f4", 4), ("u
 GRID_DTYPE = np.dtype([("origin", "<f4", 3), ("step_i", "<f4", 3), ("step_j", "<f4", 3),
                        ("step_k", "<f4", 3), ("cor_shift", "<f4"), ("scale", "<f4"),
                        ("n_i", "<i4"), ("n_j", "<i4"), ("n_k", "<i4"), ("n_views", "<i4"),
-                       ("flags", "<i4"), ("pad0", "<i4"), ("out_offset", "<i8"),
+                       ("flags", "<i4"), ("tilt", "<f4"), ("out_offset", "<i8"),
                        ("out_stride_i", "<i8"), ("out_stride_j", "<i8"), ("out_stride_k", "<i8"),
-                       ("points", "<u8"), ("pad1", "<i8"), ("mask_c", "<f8", 3),
+                       ("points", "<u8"), ("tilt_cos", "<f4"), ("tilt_sin", "<f4"), ("mask_c", "<f8", 3),
                        ("mask_ej", "<f8", 3), ("mask_ei", "<f8", 3), ("mask_half", "<f8"),
                        ("mask_delta", "<f8"), ("box", "<f8", 3), ("pad2", "<i8", 2)], align=True)
 TILE_DTYPE = np.dtype([("grid", "<i4"), ("i0", "<i4"), ("j0", "<i4"), ("k", "<i4")], align=True)
@@ -55,6 +55,8 @@ SIGNATURES = {
     "mr_plan_tiles": (ctypes.c_int, [_P, _I32, _P, _I64, ctypes.POINTER(_I64)]),
     "mr_backproject": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P]),
     "mr_backproject_staged": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P, _P]),
+    "mr_project_adjoint": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P]),
+    "mr_bp_grad_geom": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P, _P]),
     "mr_filter_f32": (ctypes.c_int, [_P, _I64, _I64, _I32, _P, _P, _P, _I32,
                                      ctypes.POINTER(MrRing), _P]),
     "mr_ingest_u16": (ctypes.c_int, [_P, _I64, _I64, _I32, _I32, _P, _P, _I32, _P, _P, _P, _I32,

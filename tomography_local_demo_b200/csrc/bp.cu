@@ -87,7 +87,6 @@ bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_st
     __syncthreads();
     const mr_grid& g = s_g;
     const int nv = g.n_views;
-    const float shift = g.cor_shift;
     const bool points = (g.flags & MR_GRID_POINTS) != 0;
 
     float acc[BP_PPT];
@@ -118,11 +117,7 @@ bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_st
                 if (tid < nch) {
                     const mr_view V = views[v0 + tid];
                     float pu[4], pv[4];
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        pu[e] = fmaf(shift, V.pw[e], V.pu[e]);
-                        pv[e] = fmaf(shift * V.uv, V.pw[e], V.pv[e]);
-                    }
+                    view_map(V, g, R, C, pu, pv);
                     s_u[tid] = make_float4(dot3(pu, ox, oy, oz) + pu[3],
                                            dot3(pu, g.step_i[0], g.step_i[1], g.step_i[2]),
                                            dot3(pu, g.step_j[0], g.step_j[1], g.step_j[2]), V.qscale);
@@ -191,13 +186,11 @@ bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_st
             __syncthreads();
             if (tid < nch) {
                 const mr_view V = views[v0 + tid];
-                float4 u, w, vq;
-                u.x = fmaf(shift, V.pw[0], V.pu[0]); u.y = fmaf(shift, V.pw[1], V.pu[1]);
-                u.z = fmaf(shift, V.pw[2], V.pu[2]); u.w = fmaf(shift, V.pw[3], V.pu[3]);
-                const float su = shift * V.uv;
-                vq.x = fmaf(su, V.pw[0], V.pv[0]); vq.y = fmaf(su, V.pw[1], V.pv[1]);
-                vq.z = fmaf(su, V.pw[2], V.pv[2]); vq.w = fmaf(su, V.pw[3], V.pv[3]);
-                w = make_float4(V.pw[0], V.pw[1], V.pw[2], V.pw[3]);
+                float pu[4], pv[4];
+                view_map(V, g, R, C, pu, pv);
+                const float4 u = make_float4(pu[0], pu[1], pu[2], pu[3]);
+                const float4 vq = make_float4(pv[0], pv[1], pv[2], pv[3]);
+                const float4 w = make_float4(V.pw[0], V.pw[1], V.pw[2], V.pw[3]);
                 s_u[tid] = u;
                 s_v[tid] = vq;
                 s_w[tid] = w;

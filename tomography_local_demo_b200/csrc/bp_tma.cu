@@ -149,15 +149,11 @@ __device__ __forceinline__ bool in_box_fp64_t(const mr_grid& g, int i, int j) {
 // Per-view footprint + local affine coefficients of one tile (computed by one lane of
 // the producer warp).
 template <int KIND, typename T>
-__device__ __forceinline__ ViewMeta view_meta(const mr_view& V, const mr_grid& g, float shift, float ox,
-                                              float oy, float oz, int di_max, int dj_max, int R, int C) {
+__device__ __forceinline__ ViewMeta view_meta(const mr_view& V, const mr_grid& g, float ox, float oy,
+                                              float oz, int di_max, int dj_max, int R, int C) {
     constexpr int W = StageGeom<T>::W;
     float pu[4], pv[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-        pu[e] = fmaf(shift, V.pw[e], V.pu[e]);
-        pv[e] = fmaf(shift * V.uv, V.pw[e], V.pv[e]);
-    }
+    view_map(V, g, R, C, pu, pv);
     auto aff = [&](const float* m) {
         return make_float3(fmaf(m[0], ox, fmaf(m[1], oy, fmaf(m[2], oz, m[3]))),
                            fmaf(m[0], g.step_i[0], fmaf(m[1], g.step_i[1], m[2] * g.step_i[2])),
@@ -292,8 +288,8 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
             const int cnt = min(32, nv - vb);
             __syncwarp();
             if (lane < cnt)
-                meta_new[lane] = view_meta<KIND, T>(views[v_begin + vb + lane], g, g.cor_shift, ox, oy, oz,
-                                                    di_max, dj_max, R, C);
+                meta_new[lane] = view_meta<KIND, T>(views[v_begin + vb + lane], g, ox, oy, oz, di_max,
+                                                    dj_max, R, C);
             __syncwarp();
             if (lane == 0) {
                 for (int l = 0; l < cnt; ++l) {

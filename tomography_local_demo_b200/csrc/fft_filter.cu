@@ -206,6 +206,76 @@ __device__ __forceinline__ void fft32xN(float2 (&v)[32], float2* buf, const floa
     }
 }
 
+// N >= 1024: passes 1 and 2 are both radix 32; they share one copy of the DIF code in a
+// runtime loop (straight-line radix-32 code is ~7 KB of SASS; four inlined copies
+// thrash the instruction cache). Same input/output contract as fft32xN.
+template <int LOG2N>
+__device__ __forceinline__ void fft_compact(float2 (&v)[32], float2* buf, const float2* __restrict__ T,
+                                            const float2* __restrict__ twN, int j) {
+    using P = Plan<LOG2N>;
+    constexpr int N = P::N, G = P::G, R3 = P::R3;
+    static_assert(P::R2 == 32, "compact path needs N >= 1024");
+    const int k = j & 31;
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+            fft_sync<G>();
+#pragma unroll
+            for (int r = 0; r < 32; ++r) {
+                float2 x = buf[pad(j + (N / 32) * r)];
+                if (r > 0) x = cmul(x, T[r * 32 + k]);
+                v[r] = x;
+            }
+        }
+        dif<32, 0, 1>(v);
+        if (pass == 0) {
+            fft_sync<G>();
+#pragma unroll
+            for (int q = 0; q < 32; ++q) buf[pad(32 * j + q)] = v[bitrev(q, 5)];
+        }
+    }
+    if constexpr (R3 == 1) {
+        float2 t[32];
+#pragma unroll
+        for (int m = 0; m < 32; ++m) t[m] = v[bitrev(m, 5)];
+#pragma unroll
+        for (int m = 0; m < 32; ++m) v[m] = t[m];
+    } else {
+        fft_sync<G>();
+#pragma unroll
+        for (int m = 0; m < 32; ++m) buf[pad((j >> 5) * 1024 + k + 32 * m)] = v[bitrev(m, 5)];
+        fft_sync<G>();
+        constexpr int NB3 = 32 / R3;
+        constexpr int L3 = ilog2(R3);
+#pragma unroll
+        for (int b = 0; b < NB3; ++b) {
+            const int jj = j + G * b;
+#pragma unroll
+            for (int r = 0; r < R3; ++r) {
+                float2 x = buf[pad(jj + (N / R3) * r)];
+                if (r > 0) x = cmul(x, __ldg(twN + r * jj));
+                v[b * R3 + r] = x;
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < NB3; ++b) dif<R3, 0, 1>(v + b * R3);
+        float2 t[32];
+#pragma unroll
+        for (int b = 0; b < NB3; ++b)
+#pragma unroll
+            for (int m = 0; m < R3; ++m) t[b + NB3 * m] = v[b * R3 + bitrev(m, L3)];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) v[q] = t[q];
+    }
+}
+
+template <int LOG2N>
+__device__ __forceinline__ void fft_any(float2 (&v)[32], float2* buf, const float2* __restrict__ T,
+                                        const float2* __restrict__ twN, int j) {
+    if constexpr (LOG2N >= 10) fft_compact<LOG2N>(v, buf, T, twN, j);
+    else fft32xN<LOG2N, false>(v, buf, T, twN, j);
+}
+
 }  // namespace fft
 
 struct Filter2Args {
@@ -267,11 +337,14 @@ __global__ void __launch_bounds__(256, LOG2N >= 11 ? 1 : 2) fft_filter_kernel(Fi
     const int R = A.rows, C = A.cols;
     const int pairs = (R + 1) / 2;
     const long long n_items = (long long)A.k * pairs;
+    // item = pair * k + view: the FPB FFT slots of a CTA take FPB views of the same row
+    // pair, so dark/gain rows are shared through L1
     for (long long base = (long long)blockIdx.x * FPB; base < n_items; base += (long long)gridDim.x * FPB) {
         const long long item = base + f;
         const bool live = item < n_items;              // uniform per FFT group
-        const int v = live ? (int)(item / pairs) : 0;
-        const int r1 = live ? 2 * (int)(item % pairs) : 0;
+        const int pr = live ? (int)(item / A.k) : 0;
+        const int v = live ? (int)(item - (long long)pr * A.k) : 0;
+        const int r1 = 2 * pr;
         const mr_filter_view fv = A.views[v];
         float2 x[32];
 #pragma unroll
@@ -294,14 +367,19 @@ __global__ void __launch_bounds__(256, LOG2N >= 11 ? 1 : 2) fft_filter_kernel(Fi
         }
 #pragma unroll
         for (int q = 16; q < 32; ++q) x[q] = make_float2(0.f, 0.f);
-        fft::fft32xN<LOG2N, true>(x, buf, T, A.tw, j);
         const float g = fv.gain * fv.out_scale;
+        // forward FFT, conj(H X), forward FFT again (= N * conj of the inverse): one call site
+#pragma unroll 1
+        for (int it = 0; it < 2; ++it) {
+            fft::fft_any<LOG2N>(x, buf, T, A.tw, j);
+            if (it == 0) {
 #pragma unroll
-        for (int q = 0; q < 32; ++q) {
-            const float h = __ldg(A.H + j + G * q) * g;
-            x[q] = make_float2(x[q].x * h, -x[q].y * h);     // conj(H X): inverse via forward FFT
+                for (int q = 0; q < 32; ++q) {
+                    const float h = __ldg(A.H + j + G * q) * g;
+                    x[q] = make_float2(x[q].x * h, -x[q].y * h);
+                }
+            }
         }
-        fft::fft32xN<LOG2N, false>(x, buf, T, A.tw, j);
         if (live) {
             const long long o1 = (long long)fv.slot * A.slot_stride + (long long)r1 * A.pitch;
             const bool two = r1 + 1 < R;

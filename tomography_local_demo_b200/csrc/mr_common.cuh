@@ -42,4 +42,29 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 
+// Per-view projective map with the grid's COR shift and detector tilt applied:
+//   no tilt: pu' = pu + shift pw,  pv' = pv + shift uv pw                 (recon.py:420)
+//   tilt   : (col, row) rotated by the tilt about the detector centre, then shifted.
+__device__ __forceinline__ void view_map(const mr_view& V, const mr_grid& g, int R, int C, float* pu,
+                                         float* pv) {
+    const float shift = g.cor_shift;
+    if (g.tilt_cos == 0.f && g.tilt_sin == 0.f) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            pu[e] = fmaf(shift, V.pw[e], V.pu[e]);
+            pv[e] = fmaf(shift * V.uv, V.pw[e], V.pv[e]);
+        }
+    } else {
+        const float c = g.tilt_cos, s = g.tilt_sin;
+        const float cc = 0.5f * (float)(C - 1), cr = 0.5f * (float)(R - 1);
+        const float ku = cc * (1.f - c) - cr * s + shift;
+        const float kv = cr * (1.f - c) + cc * s + shift * V.uv;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            pu[e] = fmaf(c, V.pu[e], fmaf(s, V.pv[e], ku * V.pw[e]));
+            pv[e] = fmaf(-s, V.pu[e], fmaf(c, V.pv[e], kv * V.pw[e]));
+        }
+    }
+}
+
 }  // namespace mr

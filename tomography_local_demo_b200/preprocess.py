@@ -23,7 +23,10 @@ def gaussian_taps(n, pad, sigma):
     f = np.fft.rfftfreq(Np)
     g = np.fft.irfft(np.exp(-2.0 * (np.pi * f * sigma) ** 2), n=Np)
     K = min(Np // 2, int(np.ceil(10.0 * sigma)) + 1)
-    return g[:K + 1]
+    taps = g[:K + 1].copy()
+    if 2 * K == Np:
+        taps[K] *= 0.5          # m = +K and m = -K are the same circular tap: count it once
+    return taps
 
 
 def _as_device(block):
