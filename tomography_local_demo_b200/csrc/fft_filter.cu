@@ -314,15 +314,28 @@ __device__ __forceinline__ float ingest_x(const Filter2Args& A, int v, int r, in
     return -__logf(fmaxf(t, 1e-3f));
 }
 
-template <int LOG2N, bool RAW>
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// PREF: the next item's two input rows are copied to shared memory with cp.async while the
+// current item's FFTs run (bin 1 only; rows of 4-byte aligned, 4-byte multiple length).
+template <int LOG2N, bool RAW, bool PREF>
 __global__ void __launch_bounds__(256, LOG2N >= 11 ? 1 : 2) fft_filter_kernel(Filter2Args A) {
     using P = fft::Plan<LOG2N>;
     constexpr int N = P::N, G = P::G, FPB = P::FPB;
+    constexpr int ES = RAW ? 2 : 4;                      // input element size
     extern __shared__ float2 sm2[];
     float2* T = sm2;                                  // 32 x 32: T[a*32+k] = W_1024^(a k)
     const int f = threadIdx.x / G;
     const int j = threadIdx.x % G;
     float2* buf = sm2 + 1024 + f * P::BUF;
+    const int row_bytes = ((A.cols * ES + 15) / 16) * 16;
+    unsigned char* pref = reinterpret_cast<unsigned char*>(sm2 + 1024 + FPB * P::BUF) + f * 2 * row_bytes;
 
     if constexpr (P::R2 > 1) {
         // W_1024^(a k) = W_N^(a k N / 1024); for N < 1024 only a multiple of 1024/N is used
@@ -337,15 +350,43 @@ __global__ void __launch_bounds__(256, LOG2N >= 11 ? 1 : 2) fft_filter_kernel(Fi
     const int R = A.rows, C = A.cols;
     const int pairs = (R + 1) / 2;
     const long long n_items = (long long)A.k * pairs;
+    const long long stride = (long long)gridDim.x * FPB;
     // item = pair * k + view: the FPB FFT slots of a CTA take FPB views of the same row
     // pair, so dark/gain rows are shared through L1
-    for (long long base = (long long)blockIdx.x * FPB; base < n_items; base += (long long)gridDim.x * FPB) {
+    auto src_row = [&](long long item, int row) -> const unsigned char* {
+        const int pr = (int)(item / A.k);
+        const int v = (int)(item - (long long)pr * A.k);
+        const int r = 2 * pr + row;
+        if (RAW) {
+            const int rr = A.flip ? (A.rows - 1 - r) : r;
+            return reinterpret_cast<const unsigned char*>(A.raw + (long long)v * A.s_view + (long long)rr * A.s_row);
+        }
+        return reinterpret_cast<const unsigned char*>(A.block + (long long)v * A.s_view + (long long)r * A.s_row);
+    };
+    auto prefetch = [&](long long item) {
+        if (PREF && item < n_items) {
+            const int units = C * ES / 4;
+            const int pr = (int)(item / A.k);
+            const int nrow = (2 * pr + 1 < R) ? 2 : 1;
+            for (int row = 0; row < nrow; ++row) {
+                const unsigned char* src = src_row(item, row);
+                for (int u = j; u < units; u += G) cp_async4(pref + row * row_bytes + 4 * u, src + 4 * u);
+            }
+        }
+        if (PREF) cp_async_commit();
+    };
+    prefetch((long long)blockIdx.x * FPB + f);
+    for (long long base = (long long)blockIdx.x * FPB; base < n_items; base += stride) {
         const long long item = base + f;
         const bool live = item < n_items;              // uniform per FFT group
         const int pr = live ? (int)(item / A.k) : 0;
         const int v = live ? (int)(item - (long long)pr * A.k) : 0;
         const int r1 = 2 * pr;
         const mr_filter_view fv = A.views[v];
+        if (PREF) {
+            cp_async_wait_all();
+            fft::fft_sync<G>();                         // the staged rows are visible to the group
+        }
         float2 x[32];
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
@@ -360,10 +401,32 @@ __global__ void __launch_bounds__(256, LOG2N >= 11 ? 1 : 2) fft_filter_kernel(Fi
                     w1 = fv.sdd * rsqrtf(fmaf(b1, b1, s2));
                     w2 = fv.sdd * rsqrtf(fmaf(b2, b2, s2));
                 }
-                a = ingest_x<RAW>(A, v, r1, c) * w1;
-                if (r1 + 1 < R) b = ingest_x<RAW>(A, v, r1 + 1, c) * w2;
+                if (PREF) {
+                    float x1, x2 = 0.f;
+                    if (RAW) {
+                        const int pix = r1 * A.cols + c;
+                        const float s1 = (float)reinterpret_cast<const uint16_t*>(pref)[c];
+                        x1 = -__logf(fmaxf((s1 - __ldg(A.dark + pix)) * __ldg(A.gain + pix), 1e-3f));
+                        if (r1 + 1 < R) {
+                            const float s2r = (float)reinterpret_cast<const uint16_t*>(pref + row_bytes)[c];
+                            x2 = -__logf(fmaxf((s2r - __ldg(A.dark + pix + A.cols)) * __ldg(A.gain + pix + A.cols), 1e-3f));
+                        }
+                    } else {
+                        x1 = reinterpret_cast<const float*>(pref)[c];
+                        if (r1 + 1 < R) x2 = reinterpret_cast<const float*>(pref + row_bytes)[c];
+                    }
+                    a = x1 * w1;
+                    b = x2 * w2;
+                } else {
+                    a = ingest_x<RAW>(A, v, r1, c) * w1;
+                    if (r1 + 1 < R) b = ingest_x<RAW>(A, v, r1 + 1, c) * w2;
+                }
             }
             x[q] = make_float2(a, b);
+        }
+        if (PREF) {
+            fft::fft_sync<G>();                         // everyone has read the staged rows
+            prefetch(item + stride);
         }
 #pragma unroll
         for (int q = 16; q < 32; ++q) x[q] = make_float2(0.f, 0.f);
@@ -411,8 +474,18 @@ __global__ void __launch_bounds__(256, LOG2N >= 11 ? 1 : 2) fft_filter_kernel(Fi
 template <int LOG2N, bool RAW>
 static int launch_fft_filter(const Filter2Args& A, cudaStream_t st) {
     using P = fft::Plan<LOG2N>;
-    const size_t smem = (1024 + (size_t)P::FPB * P::BUF) * sizeof(float2);
-    auto kern = fft_filter_kernel<LOG2N, RAW>;
+    constexpr int ES = RAW ? 2 : 4;
+    const size_t base_smem = (1024 + (size_t)P::FPB * P::BUF) * sizeof(float2);
+    const size_t row_bytes = ((size_t)A.cols * ES + 15) / 16 * 16;
+    const size_t pref_smem = (size_t)P::FPB * 2 * row_bytes;
+    // staged input rows need bin 1 and 4-byte aligned rows of a 4-byte multiple length
+    const long long elem_align = 4 / ES;
+    const bool pref = A.bin == 1 && (A.cols * ES) % 4 == 0 && A.s_view % elem_align == 0 &&
+                      A.s_row % elem_align == 0 &&
+                      (reinterpret_cast<uintptr_t>(RAW ? (const void*)A.raw : (const void*)A.block) & 3) == 0 &&
+                      base_smem + pref_smem <= 200 * 1024;
+    const size_t smem = base_smem + (pref ? pref_smem : 0);
+    auto kern = pref ? fft_filter_kernel<LOG2N, RAW, true> : fft_filter_kernel<LOG2N, RAW, false>;
     MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int dev = 0, sms = 148;
     MR_CUDA_TRY(cudaGetDevice(&dev));

@@ -864,6 +864,92 @@ class SliceReconstructor:
                     "mr_slice_entropy")
             return scores.cpu().numpy()
 
+    def bp_operator(self, requests):
+        """A differentiable back-projection (autograd.BackprojectOp) of the given slice
+        requests over the current snapshot of views; use with autograd.backproject."""
+        from .autograd import BackprojectOp
+        n_views, _, ev = self._snapshot()
+        if ev is not None:
+            torch.cuda.current_stream(self.device).wait_event(ev)
+        grids = np.zeros(len(requests), dtype=N.GRID_DTYPE)
+        off = 0
+        for r, req in enumerate(requests):
+            n = int(req.get("n", 256))
+            grids[r] = plane_grid(self.box, req["origin"], req["normal"], n, req.get("size"),
+                                  req.get("zoom", 1.0), req.get("center"), 0.0)
+            grids[r]["out_offset"] = off
+            off += n * n
+        return BackprojectOp(self._views_dev, self._kind_code, self.geom.rows, self.geom.cols, grids, off,
+                             n_views)
+
+    def calibrate(self, shift0=None, tilt0=0.0, z=0.0, n=192, fit_tilt=True, iters=60, tol=1e-3,
+                  verbose=False):
+        """Gradient-based rotation-centre / detector-tilt calibration.
+
+        Maximises a differentiable histogram score (Gaussian-kernel soft histogram of the
+        axial slice at z and of the central x-z slice, the smooth counterpart of the
+        estimate_cor criterion) over (cor_shift [px], tilt [deg]) by gradient ascent with
+        backtracking; the gradients come from the hand-written backward of the
+        back-projector. Sets the shift (tilt is returned, not stored). Returns
+        (shift, tilt_deg, history)."""
+        from .autograd import backproject, soft_neg_entropy
+        ring = self._ring
+        reqs = [dict(origin=(0.0, 0.0, z), normal=(0.0, 0.0, 1.0), n=n),
+                dict(origin=(0.0, 0.0, 0.0), normal=(0.0, 1.0, 0.0), n=n)]
+        op = self.bp_operator(reqs)
+        sizes = [n * n, n * n]
+        dev = self.device
+        deg = np.pi / 180.0
+        x = torch.tensor([self.cor_shift if shift0 is None else float(shift0), float(tilt0)],
+                         dtype=torch.float64, device=dev)
+        with torch.no_grad():
+            f0 = backproject(ring, x[0], x[1] * deg, op)
+        ranges = []
+        o = 0
+        for sz in sizes:
+            nz = f0[o:o + sz][f0[o:o + sz] != 0]
+            ranges.append((float(nz.min()), float(nz.max())) if nz.numel() else (0.0, 1.0))
+            o += sz
+
+        def score(xv, grad=True):
+            xs = xv.clone().requires_grad_(grad)
+            f = backproject(ring, xs[0], xs[1] * deg, op)
+            J, o = 0.0, 0
+            for sz, (lo, hi) in zip(sizes, ranges):
+                J = J + soft_neg_entropy(f[o:o + sz].double(), lo, hi)
+                o += sz
+            if not grad:
+                return float(J), None
+            J.backward()
+            g = xs.grad.clone()
+            if not fit_tilt:
+                g[1] = 0.0
+            return float(J), g
+
+        J, g = score(x)
+        step = 0.5
+        hist = [(float(x[0]), float(x[1]), J)]
+        for _ in range(iters):
+            d = g / max(float(g.abs().max()), 1e-30)          # unit max-norm ascent direction
+            accepted = False
+            while step > tol / 4:
+                xn = x + step * d
+                Jn, gn = score(xn)
+                if Jn > J:
+                    x, J, g = xn, Jn, gn
+                    step *= 1.5
+                    accepted = True
+                    break
+                step *= 0.5
+            hist.append((float(x[0]), float(x[1]), J))
+            if not accepted or step < tol:
+                break
+        self.set_cor_shift(float(x[0]))
+        if verbose:
+            print(f"[minirecast] calibrated COR shift {float(x[0]):+.3f} px, tilt {float(x[1]):+.4f} deg "
+                  f"({len(hist) - 1} steps)")
+        return float(x[0]), float(x[1]), hist
+
     def estimate_cor(self, shifts=None, n=192, z=0.0, verbose=True):
         """Pick the COR shift whose central axial slice has the lowest histogram entropy
         (recon.py:498-519); all trial slices go in one batched launch."""
