@@ -159,6 +159,19 @@ int mr_backproject_staged(const mr_ring* ring, const mr_view* views_dev,
                           const mr_grid* grids_dev, const mr_tile* tiles_dev, int64_t n_tiles,
                           float* out_dev, int32_t* status_dev, void* stream);
 
+/* Persistent form of mr_backproject_staged for serving: a fixed grid of CTA clusters
+ * (as many as fit on the GPU at once, at most max_tiles) pulls tile indices from a work
+ * counter until it reaches *n_tiles_dev (device int64, <= max_tiles), so the launch shape
+ * does not depend on the batch and the call can be captured in a CUDA graph once and
+ * replayed with new grid/tile contents. counter_dev: caller-provided 4-byte device
+ * scratch (4-byte aligned), zeroed on `stream` by this call; calls that share a counter
+ * must be ordered on one stream. */
+int mr_backproject_persistent(const mr_ring* ring, const mr_view* views_dev,
+                              const mr_grid* grids_dev, const mr_tile* tiles_dev,
+                              const int64_t* n_tiles_dev, int64_t max_tiles,
+                              uint32_t* counter_dev, float* out_dev, int32_t* status_dev,
+                              void* stream);
+
 /* ---- derivatives of the back-projection (no counterpart in minirecast: the reference
  * back-projector is not differentiable; the forward operator is recon.py:156-219) ----
  * Matched forward projector, the exact transpose of mr_backproject: grad_ring (F32, the
@@ -167,6 +180,13 @@ int mr_backproject_staged(const mr_ring* ring, const mr_view* views_dev,
 int mr_project_adjoint(const mr_ring* grad_ring, const mr_view* views_dev,
                        const mr_grid* grids_dev, const mr_tile* tiles_dev, int64_t n_tiles,
                        const float* grad_out_dev, void* stream);
+
+/* The forward operator of the differentiable path: the same result as mr_backproject,
+ * computed with the coordinate arithmetic of mr_project_adjoint / mr_bp_grad_geom, so
+ * that the adjoint is its transpose to the rounding of the sums. */
+int mr_backproject_matched(const mr_ring* ring, const mr_view* views_dev,
+                           const mr_grid* grids_dev, const mr_tile* tiles_dev, int64_t n_tiles,
+                           float* out_dev, void* stream);
 
 /* dgeom[2*g + 0] += d<grad_out, f_g>/d cor_shift, dgeom[2*g + 1] += d<...>/d tilt (per
  * radian) for every grid g, with f the forward output of mr_backproject on `ring`.

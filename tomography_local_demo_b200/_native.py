@@ -55,6 +55,8 @@ SIGNATURES = {
     "mr_plan_tiles": (ctypes.c_int, [_P, _I32, _P, _I64, ctypes.POINTER(_I64)]),
     "mr_backproject": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P]),
     "mr_backproject_staged": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P, _P]),
+    "mr_backproject_persistent": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _P, _I64, _P, _P, _P, _P]),
+    "mr_backproject_matched": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P]),
     "mr_project_adjoint": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P]),
     "mr_bp_grad_geom": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P, _P]),
     "mr_filter_f32": (ctypes.c_int, [_P, _I64, _I64, _I32, _P, _P, _P, _I32,

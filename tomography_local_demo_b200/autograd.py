@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-from .recon import _ring_struct, _struct_tensor, backproject_device, ctypes_void
+from .recon import _ring_struct, _struct_tensor, ctypes_void
 
 _CODES = {torch.float32: N.MR_F32, torch.bfloat16: N.MR_BF16, torch.float16: N.MR_F16}
 
@@ -66,10 +66,15 @@ class BackprojectOp:
         return _ring_struct(q, _CODES[q.dtype], self.kind, self.rows, self.cols)
 
     def forward(self, q, shift=0.0, tilt=0.0):
+        """B q with the coordinate arithmetic of the backward kernels (mr_backproject_matched)."""
         out = torch.zeros(self.n_out, dtype=torch.float32, device=self.device)
+        grids = self.grids_at(shift, tilt)
+        g_dev, t_dev = self._tiles(grids)
         st = torch.cuda.current_stream(self.device)
-        backproject_device(self._ring(q), self.views, self.grids_at(shift, tilt), out, st, self.device,
-                           kernel="plain")
+        v = ctypes_void
+        N.check(N.load().mr_backproject_matched(self._ring(q), v(self.views.data_ptr()), v(g_dev.data_ptr()),
+                                                v(t_dev.data_ptr()), t_dev.numel() // N.TILE_DTYPE.itemsize,
+                                                v(out.data_ptr()), v(st.cuda_stream)), "mr_backproject_matched")
         return out
 
     def _tiles(self, grids):

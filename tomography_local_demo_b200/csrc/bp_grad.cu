@@ -5,6 +5,9 @@
 //                        upstream gradient g[p] is scattered to the same four bilinear taps,
 //                        with the same weights, that the forward kernel gathers from (the
 //                        exact transpose, taps outside the detector dropped as in forward).
+//   mr_backproject_matched : the forward B q with exactly the coordinate arithmetic of
+//                        the two kernels below (its transpose is mr_project_adjoint to
+//                        the last rounding of the sums);
 //   mr_bp_grad_geom    : d<g, f>/d shift and d<g, f>/d tilt per grid, from the analytic
 //                        derivative of the bilinear interpolant:
 //                          dv/dcol = (1-fr)(q01-q00) + fr (q11-q10)
@@ -20,7 +23,7 @@ constexpr int GR_THREADS = 256;
 constexpr int GR_PPT = 4;
 constexpr int GR_VCH = 128;
 
-enum : int { GRAD_ADJOINT = 0, GRAD_GEOM = 1 };
+enum : int { GRAD_ADJOINT = 0, GRAD_GEOM = 1, GRAD_FORWARD = 2 };
 
 template <int KIND, int MODE, typename T>
 __global__ void __launch_bounds__(GR_THREADS)
@@ -42,7 +45,9 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
     const int tx = ((warp & 3) << 3) | (lane & 7);
     const int ty = ((warp >> 2) << 4) | (lane >> 3);
 
-    float px[GR_PPT], py[GR_PPT], pz[GR_PPT], gp[GR_PPT];
+    float px[GR_PPT], py[GR_PPT], pz[GR_PPT], gp[GR_PPT], acc[GR_PPT];
+    long long oidx[GR_PPT];
+    bool live[GR_PPT];
 #pragma unroll
     for (int p = 0; p < GR_PPT; ++p) {
         int i, j;
@@ -71,7 +76,10 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
                 inside = inside && (fabs(q) <= g.box[e]);
             }
         }
-        gp[p] = inside ? gout[o] * g.scale : 0.f;
+        live[p] = inside;
+        oidx[p] = o;
+        acc[p] = 0.f;
+        gp[p] = (MODE != GRAD_FORWARD && inside) ? gout[o] * g.scale : 0.f;
         if (pts) {
             const int jj = ok ? j : 0;
             px[p] = g.points[3 * jj];
@@ -107,7 +115,7 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
             const long long slot = (long long)(v0 + vv) * slot_stride;
 #pragma unroll
             for (int p = 0; p < GR_PPT; ++p) {
-                if (gp[p] == 0.f) continue;
+                if (MODE == GRAD_FORWARD ? !live[p] : gp[p] == 0.f) continue;
                 float col = fmaf(cu.x, px[p], fmaf(cu.y, py[p], fmaf(cu.z, pz[p], cu.w)));
                 float row = fmaf(cv.x, px[p], fmaf(cv.y, py[p], fmaf(cv.z, pz[p], cv.w)));
                 float w = qs;
@@ -125,7 +133,15 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
                 const bool ri0 = (unsigned)r0 < (unsigned)R, ri1 = (unsigned)(r0 + 1) < (unsigned)R;
                 const bool ci0 = (unsigned)c0 < (unsigned)C, ci1 = (unsigned)(c0 + 1) < (unsigned)C;
                 const long long base = slot + (long long)r0 * pitch + c0;
-                if (MODE == GRAD_ADJOINT) {
+                if (MODE == GRAD_FORWARD) {
+                    const float q00 = (ri0 && ci0) ? ld_elem(ring + base) : 0.f;
+                    const float q01 = (ri0 && ci1) ? ld_elem(ring + base + 1) : 0.f;
+                    const float q10 = (ri1 && ci0) ? ld_elem(ring + base + pitch) : 0.f;
+                    const float q11 = (ri1 && ci1) ? ld_elem(ring + base + pitch + 1) : 0.f;
+                    const float a = fmaf(fc, q01 - q00, q00);
+                    const float b = fmaf(fc, q11 - q10, q10);
+                    acc[p] = fmaf(w, fmaf(fr, b - a, a), acc[p]);
+                } else if (MODE == GRAD_ADJOINT) {
                     const float a = w * gp[p];
                     if (ri0 && ci0) atomicAdd(gring + base, a * (1.f - fr) * (1.f - fc));
                     if (ri0 && ci1) atomicAdd(gring + base + 1, a * (1.f - fr) * fc);
@@ -145,6 +161,14 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
                     dt = fmaf(a, dcol * (row - shift * uv - cr) - drow * (col - shift - cc), dt);
                 }
             }
+        }
+    }
+    if (MODE == GRAD_FORWARD) {
+#pragma unroll
+        for (int p = 0; p < GR_PPT; ++p) {
+            const bool ok = pts ? (t.j0 + tid + GR_THREADS * p < g.n_j)
+                                : (t.i0 + ty + 4 * p < g.n_i && t.j0 + tx < g.n_j);
+            if (ok) gring[oidx[p]] = live[p] ? acc[p] * g.scale : 0.f;
         }
     }
     if (MODE == GRAD_GEOM) {
@@ -202,6 +226,36 @@ extern "C" int mr_project_adjoint(const mr_ring* grad_ring, const mr_view* views
                                                                   grad_out, nullptr, st)
                : mr::launch_grad<MR_PARALLEL, mr::GRAD_ADJOINT, float>(grad_ring, g, views, grids, tiles,
                                                                       n_tiles, grad_out, nullptr, st);
+}
+
+extern "C" int mr_backproject_matched(const mr_ring* ring, const mr_view* views, const mr_grid* grids,
+                                      const mr_tile* tiles, int64_t n_tiles, float* out, void* stream) {
+    int rc = mr::check_ring(ring);
+    if (rc != MR_OK) return rc;
+    if (!views || !grids || !out || n_tiles < 0 || (n_tiles > 0 && !tiles)) return MR_ERR_INVALID;
+    if (n_tiles == 0) return MR_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool cone = ring->kind == MR_CONE;
+    switch (ring->dtype) {
+        case MR_F32:
+            return cone ? mr::launch_grad<MR_CONE, mr::GRAD_FORWARD, float>(ring, out, views, grids, tiles, n_tiles,
+                                                                           nullptr, nullptr, st)
+                        : mr::launch_grad<MR_PARALLEL, mr::GRAD_FORWARD, float>(ring, out, views, grids, tiles,
+                                                                               n_tiles, nullptr, nullptr, st);
+        case MR_BF16:
+            return cone ? mr::launch_grad<MR_CONE, mr::GRAD_FORWARD, __nv_bfloat16>(ring, out, views, grids, tiles,
+                                                                                   n_tiles, nullptr, nullptr, st)
+                        : mr::launch_grad<MR_PARALLEL, mr::GRAD_FORWARD, __nv_bfloat16>(ring, out, views, grids,
+                                                                                       tiles, n_tiles, nullptr,
+                                                                                       nullptr, st);
+        case MR_F16:
+            return cone ? mr::launch_grad<MR_CONE, mr::GRAD_FORWARD, __half>(ring, out, views, grids, tiles, n_tiles,
+                                                                            nullptr, nullptr, st)
+                        : mr::launch_grad<MR_PARALLEL, mr::GRAD_FORWARD, __half>(ring, out, views, grids, tiles,
+                                                                                n_tiles, nullptr, nullptr, st);
+        default:
+            return MR_ERR_INVALID;
+    }
 }
 
 extern "C" int mr_bp_grad_geom(const mr_ring* ring, const mr_view* views, const mr_grid* grids,

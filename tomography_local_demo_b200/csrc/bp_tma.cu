@@ -224,7 +224,8 @@ __global__ void __launch_bounds__(ST_THREADS)
 bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__ ring, int R, int C,
                  int pitch, long long slot_stride, const mr_view* __restrict__ views,
                  const mr_grid* __restrict__ grids, const mr_tile* __restrict__ tiles,
-                 float* __restrict__ out, int* status) {
+                 float* __restrict__ out, int* status, const int64_t* __restrict__ n_tiles_dev,
+                 unsigned int* __restrict__ counter) {
     constexpr int W = StageGeom<T>::W;
     constexpr int S = StageGeom<T>::STAGES;
     constexpr int ESZ = (int)sizeof(T);
@@ -246,161 +247,185 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
     cg::cluster_group cluster = cg::this_cluster();
     const int crank = (int)cluster.block_rank();
     const int csize = (int)cluster.num_blocks();
-    const mr_tile t = tiles[blockIdx.x / csize];
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const bool producer = warp == ST_CONSUMERS;
-    if (tid < (int)(sizeof(mr_grid) / 4))
-        reinterpret_cast<int*>(&s_g)[tid] = reinterpret_cast<const int*>(grids + t.grid)[tid];
+    __shared__ unsigned int s_next;
     if (tid < S) {
         mbar_init(&full[tid], 1);
         mbar_init(&empty[tid], ST_CONSUMERS);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     __syncthreads();
-    const mr_grid& g = s_g;
-    // this CTA's share of the views: [v_begin, v_end)
-    const int v_begin = (int)(((long long)g.n_views * crank) / csize);
-    const int v_end = (int)(((long long)g.n_views * (crank + 1)) / csize);
-    const int nv = v_end - v_begin;
+    uint32_t used = 0;              // views this CTA has put through the stage ring so far
 
-    const float ox = g.origin[0] + t.i0 * g.step_i[0] + t.j0 * g.step_j[0] + t.k * g.step_k[0];
-    const float oy = g.origin[1] + t.i0 * g.step_i[1] + t.j0 * g.step_j[1] + t.k * g.step_k[1];
-    const float oz = g.origin[2] + t.i0 * g.step_i[2] + t.j0 * g.step_j[2] + t.k * g.step_k[2];
-    const int tx = ((warp & 3) << 3) | (lane & 7);
-    const int ty = ((warp >> 2) << 4) | (lane >> 3);
-    bool inside[ST_PPT];
-    bool any = false;
-#pragma unroll
-    for (int p = 0; p < ST_PPT; ++p) {
-        const int i = t.i0 + ty + 4 * p, j = t.j0 + tx;
-        bool ok = !producer && i < g.n_i && j < g.n_j;
-        if (ok && (g.flags & MR_GRID_MASK_BOX)) ok = in_box_fp64_t(g, i, j);
-        inside[p] = ok;
-        any |= ok;
-    }
-    const bool tile_live = __syncthreads_or(any) != 0;
+    // One tile per cluster (counter == nullptr), or persistent: clusters pull tile indices
+    // from the device work counter until it passes *n_tiles_dev.
+    for (int iter = 0;; ++iter) {
+        int tile_idx;
+        if (counter) {
+            if (crank == 0 && tid == 0) s_next = atomicAdd(counter, 1u);
+            cluster.sync();
+            tile_idx = (int)*cluster.map_shared_rank(&s_next, 0);
+            if ((int64_t)tile_idx >= *n_tiles_dev) break;
+        } else {
+            if (iter > 0) break;
+            tile_idx = (int)(blockIdx.x / csize);
+        }
+        const mr_tile t = tiles[tile_idx];
+        __syncthreads();                    // previous tile's readers of s_g are done
+        if (tid < (int)(sizeof(mr_grid) / 4))
+            reinterpret_cast<int*>(&s_g)[tid] = reinterpret_cast<const int*>(grids + t.grid)[tid];
+        __syncthreads();
+        const mr_grid& g = s_g;
+        // this CTA's share of the views: [v_begin, v_end)
+        const int v_begin = (int)(((long long)g.n_views * crank) / csize);
+        const int v_end = (int)(((long long)g.n_views * (crank + 1)) / csize);
+        const int nv = v_end - v_begin;
 
-    if (producer && tile_live) {
-        const int di_max = min(ST_TI, g.n_i - t.i0) - 1;
-        const int dj_max = min(ST_TJ, g.n_j - t.j0) - 1;
-        for (int vb = 0; vb < nv; vb += 32) {
-            const int cnt = min(32, nv - vb);
-            __syncwarp();
-            if (lane < cnt)
-                meta_new[lane] = view_meta<KIND, T>(views[v_begin + vb + lane], g, ox, oy, oz, di_max,
-                                                    dj_max, R, C);
-            __syncwarp();
-            if (lane == 0) {
-                for (int l = 0; l < cnt; ++l) {
-                    const int v = vb + l, s = v % S, u = v / S;
-                    if (u > 0) mbar_wait(&empty[s], (u - 1) & 1, status);
-                    const ViewMeta m = meta_new[l];
-                    meta_ring[s] = m;
-                    if (m.mode == MODE_STAGED) {
-                        mbar_arrive_tx(&full[s], (uint32_t)(m.nbox * BOX_BYTES));
-                        unsigned char* dst = stages + s * STAGE_BYTES;
-                        for (int b = 0; b < m.nbox; ++b)
-                            tma_load_3d(dst + b * BOX_BYTES, &tmap, m.x0, m.r0 + b * ST_BOX_H, v_begin + v,
-                                        &full[s]);
-                    } else {
-                        mbar_arrive(&full[s]);
-                    }
-                }
-            }
-        }
-    }
-
-    float acc[ST_PPT];
-#pragma unroll
-    for (int p = 0; p < ST_PPT; ++p) acc[p] = 0.f;
-    if (!producer && tile_live) {
-        const float fj = (float)tx;
-        for (int v = 0; v < nv; ++v) {
-            const int s = v % S;
-            mbar_wait(&full[s], (uint32_t)((v / S) & 1), status);
-            const ViewMeta m = meta_ring[s];
-            const float bu = fmaf(fj, m.cu.z, m.cu.x);
-            const float bv = fmaf(fj, m.cv.z, m.cv.x);
-            const float bw = fmaf(fj, m.cw.z, m.cw.x);
-            if (m.mode == MODE_STAGED) {
-                const uint32_t base = smem_u32(stages + s * STAGE_BYTES);
-                const uint32_t maxoff = (uint32_t)(m.nbox * BOX_BYTES - (W + 1) * ESZ - ESZ);
-                // byte offset = (bits_r - MAGIC_BITS) * W*ESZ + (bits_c - MAGIC_BITS) * ESZ
-                const uint32_t kofs = (uint32_t)MAGIC_BITS * (uint32_t)(W * ESZ + ESZ);
-#pragma unroll
-                for (int p = 0; p < ST_PPT; ++p) {
-                    const float fi = (float)(ty + 4 * p);
-                    const float nu = fmaf(fi, m.cu.y, bu);
-                    const float nvv = fmaf(fi, m.cv.y, bv);
-                    float r = 1.f, yc, yr, fc, fr;
-                    if (KIND == MR_CONE) {
-                        r = rcp_approx(fmaf(fi, m.cw.y, bw));
-                        yc = __fmaf_rd(nu, r, MAGIC);
-                        yr = __fmaf_rd(nvv, r, MAGIC);
-                        fc = fmaf(nu, r, MAGIC - yc);
-                        fr = fmaf(nvv, r, MAGIC - yr);
-                    } else {
-                        yc = __fadd_rd(nu, MAGIC);
-                        yr = __fadd_rd(nvv, MAGIC);
-                        fc = nu + (MAGIC - yc);
-                        fr = nvv + (MAGIC - yr);
-                    }
-                    uint32_t off = (uint32_t)__float_as_int(yr) * (uint32_t)(W * ESZ) +
-                                   (uint32_t)__float_as_int(yc) * (uint32_t)ESZ - kofs;
-                    off = min(off, maxoff);
-                    const uint32_t a = base + off;
-                    const float q00 = lds_elem<T>(a);
-                    const float q01 = lds_elem<T>(a + ESZ);
-                    const float q10 = lds_elem<T>(a + W * ESZ);
-                    const float q11 = lds_elem<T>(a + W * ESZ + ESZ);
-                    const float ta = fmaf(fc, q01 - q00, q00);
-                    const float tb = fmaf(fc, q11 - q10, q10);
-                    const float val = fmaf(fr, tb - ta, ta);
-                    acc[p] = fmaf(KIND == MR_CONE ? r * r : m.cu.w, val, acc[p]);
-                }
-            } else if (m.mode == MODE_GLOBAL) {
-                const T* q = ring + (long long)(v_begin + v) * slot_stride;
-#pragma unroll
-                for (int p = 0; p < ST_PPT; ++p) {
-                    const float fi = (float)(ty + 4 * p);
-                    const float nu = fmaf(fi, m.cu.y, bu);
-                    const float nvv = fmaf(fi, m.cv.y, bv);
-                    if (KIND == MR_CONE) {
-                        const float r = rcp_approx(fmaf(fi, m.cw.y, bw));
-                        acc[p] = fmaf(r * r, bilerp_global(q, R, C, pitch, nvv * r, nu * r), acc[p]);
-                    } else {
-                        acc[p] = fmaf(m.cu.w, bilerp_global(q, R, C, pitch, nvv, nu), acc[p]);
-                    }
-                }
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[s]);      // this warp is done with stage s
-        }
-    }
-    // ---- cluster reduction of the view-quarter partial sums (rank order), rank 0 writes
-    if (csize > 1) {
-        if (!producer) partial[tid] = make_float4(acc[0], acc[1], acc[2], acc[3]);
-        cluster.sync();
-        if (crank == 0 && !producer) {
-            for (int r = 1; r < csize; ++r) {
-                const float4 o = cluster.map_shared_rank(partial, r)[tid];
-                acc[0] += o.x; acc[1] += o.y; acc[2] += o.z; acc[3] += o.w;
-            }
-        }
-    }
-    if (crank == 0 && !producer) {
+        const float ox = g.origin[0] + t.i0 * g.step_i[0] + t.j0 * g.step_j[0] + t.k * g.step_k[0];
+        const float oy = g.origin[1] + t.i0 * g.step_i[1] + t.j0 * g.step_j[1] + t.k * g.step_k[1];
+        const float oz = g.origin[2] + t.i0 * g.step_i[2] + t.j0 * g.step_j[2] + t.k * g.step_k[2];
+        const int tx = ((warp & 3) << 3) | (lane & 7);
+        const int ty = ((warp >> 2) << 4) | (lane >> 3);
+        bool inside[ST_PPT];
+        bool any = false;
 #pragma unroll
         for (int p = 0; p < ST_PPT; ++p) {
             const int i = t.i0 + ty + 4 * p, j = t.j0 + tx;
-            if (i < g.n_i && j < g.n_j) {
-                const long long o = g.out_offset + (long long)i * g.out_stride_i +
-                                    (long long)j * g.out_stride_j + (long long)t.k * g.out_stride_k;
-                out[o] = inside[p] ? acc[p] * g.scale : 0.f;
+            bool ok = !producer && i < g.n_i && j < g.n_j;
+            if (ok && (g.flags & MR_GRID_MASK_BOX)) ok = in_box_fp64_t(g, i, j);
+            inside[p] = ok;
+            any |= ok;
+        }
+        const bool tile_live = __syncthreads_or(any) != 0;
+
+        if (producer && tile_live) {
+            const int di_max = min(ST_TI, g.n_i - t.i0) - 1;
+            const int dj_max = min(ST_TJ, g.n_j - t.j0) - 1;
+            for (int vb = 0; vb < nv; vb += 32) {
+                const int cnt = min(32, nv - vb);
+                __syncwarp();
+                if (lane < cnt)
+                    meta_new[lane] = view_meta<KIND, T>(views[v_begin + vb + lane], g, ox, oy, oz, di_max,
+                                                        dj_max, R, C);
+                __syncwarp();
+                if (lane == 0) {
+                    for (int l = 0; l < cnt; ++l) {
+                        const uint32_t ua = used + (uint32_t)(vb + l);      // absolute stage use
+                        const int s = (int)(ua % S);
+                        const uint32_t u = ua / S;
+                        if (u > 0) mbar_wait(&empty[s], (u - 1) & 1u, status);
+                        const ViewMeta m = meta_new[l];
+                        meta_ring[s] = m;
+                        if (m.mode == MODE_STAGED) {
+                            mbar_arrive_tx(&full[s], (uint32_t)(m.nbox * BOX_BYTES));
+                            unsigned char* dst = stages + s * STAGE_BYTES;
+                            for (int b = 0; b < m.nbox; ++b)
+                                tma_load_3d(dst + b * BOX_BYTES, &tmap, m.x0, m.r0 + b * ST_BOX_H,
+                                            v_begin + vb + l, &full[s]);
+                        } else {
+                            mbar_arrive(&full[s]);
+                        }
+                    }
+                }
             }
         }
+
+        float acc[ST_PPT];
+#pragma unroll
+        for (int p = 0; p < ST_PPT; ++p) acc[p] = 0.f;
+        if (!producer && tile_live) {
+            const float fj = (float)tx;
+            for (int v = 0; v < nv; ++v) {
+                const uint32_t ua = used + (uint32_t)v;
+                const int s = (int)(ua % S);
+                mbar_wait(&full[s], (ua / S) & 1u, status);
+                const ViewMeta m = meta_ring[s];
+                const float bu = fmaf(fj, m.cu.z, m.cu.x);
+                const float bv = fmaf(fj, m.cv.z, m.cv.x);
+                const float bw = fmaf(fj, m.cw.z, m.cw.x);
+                if (m.mode == MODE_STAGED) {
+                    const uint32_t base = smem_u32(stages + s * STAGE_BYTES);
+                    const uint32_t maxoff = (uint32_t)(m.nbox * BOX_BYTES - (W + 1) * ESZ - ESZ);
+                    // byte offset = (bits_r - MAGIC_BITS) * W*ESZ + (bits_c - MAGIC_BITS) * ESZ
+                    const uint32_t kofs = (uint32_t)MAGIC_BITS * (uint32_t)(W * ESZ + ESZ);
+#pragma unroll
+                    for (int p = 0; p < ST_PPT; ++p) {
+                        const float fi = (float)(ty + 4 * p);
+                        const float nu = fmaf(fi, m.cu.y, bu);
+                        const float nvv = fmaf(fi, m.cv.y, bv);
+                        float r = 1.f, yc, yr, fc, fr;
+                        if (KIND == MR_CONE) {
+                            r = rcp_approx(fmaf(fi, m.cw.y, bw));
+                            yc = __fmaf_rd(nu, r, MAGIC);
+                            yr = __fmaf_rd(nvv, r, MAGIC);
+                            fc = fmaf(nu, r, MAGIC - yc);
+                            fr = fmaf(nvv, r, MAGIC - yr);
+                        } else {
+                            yc = __fadd_rd(nu, MAGIC);
+                            yr = __fadd_rd(nvv, MAGIC);
+                            fc = nu + (MAGIC - yc);
+                            fr = nvv + (MAGIC - yr);
+                        }
+                        uint32_t off = (uint32_t)__float_as_int(yr) * (uint32_t)(W * ESZ) +
+                                       (uint32_t)__float_as_int(yc) * (uint32_t)ESZ - kofs;
+                        off = min(off, maxoff);
+                        const uint32_t a = base + off;
+                        const float q00 = lds_elem<T>(a);
+                        const float q01 = lds_elem<T>(a + ESZ);
+                        const float q10 = lds_elem<T>(a + W * ESZ);
+                        const float q11 = lds_elem<T>(a + W * ESZ + ESZ);
+                        const float ta = fmaf(fc, q01 - q00, q00);
+                        const float tb = fmaf(fc, q11 - q10, q10);
+                        const float val = fmaf(fr, tb - ta, ta);
+                        acc[p] = fmaf(KIND == MR_CONE ? r * r : m.cu.w, val, acc[p]);
+                    }
+                } else if (m.mode == MODE_GLOBAL) {
+                    const T* q = ring + (long long)(v_begin + v) * slot_stride;
+#pragma unroll
+                    for (int p = 0; p < ST_PPT; ++p) {
+                        const float fi = (float)(ty + 4 * p);
+                        const float nu = fmaf(fi, m.cu.y, bu);
+                        const float nvv = fmaf(fi, m.cv.y, bv);
+                        if (KIND == MR_CONE) {
+                            const float r = rcp_approx(fmaf(fi, m.cw.y, bw));
+                            acc[p] = fmaf(r * r, bilerp_global(q, R, C, pitch, nvv * r, nu * r), acc[p]);
+                        } else {
+                            acc[p] = fmaf(m.cu.w, bilerp_global(q, R, C, pitch, nvv, nu), acc[p]);
+                        }
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[s]);      // this warp is done with stage s
+            }
+        }
+        if (tile_live) used += (uint32_t)nv;
+
+        // ---- cluster reduction of the view-quarter partial sums (rank order), rank 0 writes
+        if (csize > 1) {
+            if (!producer) partial[tid] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+            cluster.sync();
+            if (crank == 0 && !producer) {
+                for (int r = 1; r < csize; ++r) {
+                    const float4 o = cluster.map_shared_rank(partial, r)[tid];
+                    acc[0] += o.x; acc[1] += o.y; acc[2] += o.z; acc[3] += o.w;
+                }
+            }
+        }
+        if (crank == 0 && !producer) {
+#pragma unroll
+            for (int p = 0; p < ST_PPT; ++p) {
+                const int i = t.i0 + ty + 4 * p, j = t.j0 + tx;
+                if (i < g.n_i && j < g.n_j) {
+                    const long long o = g.out_offset + (long long)i * g.out_stride_i +
+                                        (long long)j * g.out_stride_j + (long long)t.k * g.out_stride_k;
+                    out[o] = inside[p] ? acc[p] * g.scale : 0.f;
+                }
+            }
+        }
+        if (csize > 1) cluster.sync();      // keep every partial alive until rank 0 has read it
     }
-    if (csize > 1) cluster.sync();          // keep every partial alive until rank 0 has read it
 }
 
 // ---------------------------------------------------------------- host side
@@ -437,7 +462,8 @@ static int make_ring_map(const mr_ring* ring, CUtensorMap* map) {
 
 template <int KIND, typename T>
 static int launch_staged(const mr_ring* ring, const mr_view* views, const mr_grid* grids,
-                         const mr_tile* tiles, int64_t n_tiles, float* out, int* status, cudaStream_t st) {
+                         const mr_tile* tiles, int64_t n_tiles, float* out, int* status, cudaStream_t st,
+                         const int64_t* n_tiles_dev = nullptr, unsigned int* counter = nullptr) {
     CUtensorMap map;
     int rc = make_ring_map<T>(ring, &map);
     if (rc != MR_OK) return rc;
@@ -447,27 +473,69 @@ static int launch_staged(const mr_ring* ring, const mr_view* views, const mr_gri
                         ST_CONSUMERS * 32 * sizeof(float4) + 128;
     auto kern = bp_staged_kernel<KIND, T>;
     MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int64_t max_chunk = 2147483647LL / ST_CLUSTER;
-    for (int64_t t0 = 0; t0 < n_tiles; t0 += max_chunk) {
-        const int64_t n = (n_tiles - t0) < max_chunk ? (n_tiles - t0) : max_chunk;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(n * ST_CLUSTER));
-        cfg.blockDim = dim3(ST_THREADS);
-        cfg.dynamicSmemBytes = smem;
-        cfg.stream = st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = ST_CLUSTER;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        MR_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, map, static_cast<const T*>(ring->data), ring->rows,
-                                       ring->cols, ring->col_pitch, (long long)ring->slot_stride, views, grids,
-                                       tiles + t0, out, status));
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(ST_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = ST_CLUSTER;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (counter) {
+        // persistent: as many clusters as fit at once, pulling tiles from the counter
+        int clusters = 0;
+        cfg.gridDim = dim3(ST_CLUSTER);
+        MR_CUDA_TRY(cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg));
+        if (clusters < 1) clusters = 1;
+        if ((int64_t)clusters > n_tiles) clusters = (int)(n_tiles > 0 ? n_tiles : 1);
+        MR_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), st));
+        cfg.gridDim = dim3((unsigned)(clusters * ST_CLUSTER));
+        MR_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, map, static_cast<const T*>(ring->data), ring->rows, ring->cols,
+                                       ring->col_pitch, (long long)ring->slot_stride, views, grids, tiles, out,
+                                       status, n_tiles_dev, counter));
+    } else {
+        const int64_t max_chunk = 2147483647LL / ST_CLUSTER;
+        for (int64_t t0 = 0; t0 < n_tiles; t0 += max_chunk) {
+            const int64_t n = (n_tiles - t0) < max_chunk ? (n_tiles - t0) : max_chunk;
+            cfg.gridDim = dim3((unsigned)(n * ST_CLUSTER));
+            MR_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, map, static_cast<const T*>(ring->data), ring->rows,
+                                           ring->cols, ring->col_pitch, (long long)ring->slot_stride, views,
+                                           grids, tiles + t0, out, status, (const int64_t*)nullptr,
+                                           (unsigned int*)nullptr));
+        }
     }
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;
+}
+
+static int check_staged_ring(const mr_ring* ring) {
+    if (!ring || !ring->data) return MR_ERR_INVALID;
+    if (ring->rows <= 0 || ring->cols <= 0 || ring->col_pitch < ring->cols || ring->n_slots <= 0)
+        return MR_ERR_INVALID;
+    if (ring->slot_stride < (int64_t)ring->rows * ring->col_pitch) return MR_ERR_INVALID;
+    if (ring->kind != MR_CONE && ring->kind != MR_PARALLEL) return MR_ERR_INVALID;
+    if ((reinterpret_cast<uintptr_t>(ring->data) & 15) != 0) return MR_ERR_INVALID;
+    const int esz = ring->dtype == MR_F32 ? 4 : 2;
+    if (ring->dtype != MR_F32 && ring->dtype != MR_BF16 && ring->dtype != MR_F16) return MR_ERR_INVALID;
+    if ((ring->col_pitch * esz) % 16 || (ring->slot_stride * esz) % 16) return MR_ERR_INVALID;
+    return MR_OK;
+}
+
+template <typename... Args>
+static int dispatch_staged(const mr_ring* ring, Args... args) {
+    const bool cone = ring->kind == MR_CONE;
+    switch (ring->dtype) {
+        case MR_F32:
+            return cone ? launch_staged<MR_CONE, float>(ring, args...) : launch_staged<MR_PARALLEL, float>(ring, args...);
+        case MR_BF16:
+            return cone ? launch_staged<MR_CONE, __nv_bfloat16>(ring, args...)
+                        : launch_staged<MR_PARALLEL, __nv_bfloat16>(ring, args...);
+        default:
+            return cone ? launch_staged<MR_CONE, __half>(ring, args...) : launch_staged<MR_PARALLEL, __half>(ring, args...);
+    }
 }
 
 }  // namespace mr
@@ -475,30 +543,21 @@ static int launch_staged(const mr_ring* ring, const mr_view* views, const mr_gri
 extern "C" int mr_backproject_staged(const mr_ring* ring, const mr_view* views, const mr_grid* grids,
                                      const mr_tile* tiles, int64_t n_tiles, float* out, int32_t* status,
                                      void* stream) {
-    if (!ring || !ring->data || !views || !grids || !out || n_tiles < 0) return MR_ERR_INVALID;
-    if (n_tiles > 0 && !tiles) return MR_ERR_INVALID;
-    if (ring->rows <= 0 || ring->cols <= 0 || ring->col_pitch < ring->cols || ring->n_slots <= 0)
-        return MR_ERR_INVALID;
-    if (ring->slot_stride < (int64_t)ring->rows * ring->col_pitch) return MR_ERR_INVALID;
-    if (ring->kind != MR_CONE && ring->kind != MR_PARALLEL) return MR_ERR_INVALID;
-    if ((reinterpret_cast<uintptr_t>(ring->data) & 15) != 0) return MR_ERR_INVALID;
+    int rc = mr::check_staged_ring(ring);
+    if (rc != MR_OK) return rc;
+    if (!views || !grids || !out || n_tiles < 0 || (n_tiles > 0 && !tiles)) return MR_ERR_INVALID;
     if (n_tiles == 0) return MR_OK;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const bool cone = ring->kind == MR_CONE;
-    switch (ring->dtype) {
-        case MR_F32:
-            if ((ring->col_pitch * 4) % 16 || (ring->slot_stride * 4) % 16) return MR_ERR_INVALID;
-            return cone ? mr::launch_staged<MR_CONE, float>(ring, views, grids, tiles, n_tiles, out, status, st)
-                        : mr::launch_staged<MR_PARALLEL, float>(ring, views, grids, tiles, n_tiles, out, status, st);
-        case MR_BF16:
-            if ((ring->col_pitch * 2) % 16 || (ring->slot_stride * 2) % 16) return MR_ERR_INVALID;
-            return cone ? mr::launch_staged<MR_CONE, __nv_bfloat16>(ring, views, grids, tiles, n_tiles, out, status, st)
-                        : mr::launch_staged<MR_PARALLEL, __nv_bfloat16>(ring, views, grids, tiles, n_tiles, out, status, st);
-        case MR_F16:
-            if ((ring->col_pitch * 2) % 16 || (ring->slot_stride * 2) % 16) return MR_ERR_INVALID;
-            return cone ? mr::launch_staged<MR_CONE, __half>(ring, views, grids, tiles, n_tiles, out, status, st)
-                        : mr::launch_staged<MR_PARALLEL, __half>(ring, views, grids, tiles, n_tiles, out, status, st);
-        default:
-            return MR_ERR_INVALID;
-    }
+    return mr::dispatch_staged(ring, views, grids, tiles, n_tiles, out, status, static_cast<cudaStream_t>(stream),
+                               (const int64_t*)nullptr, (unsigned int*)nullptr);
+}
+
+extern "C" int mr_backproject_persistent(const mr_ring* ring, const mr_view* views, const mr_grid* grids,
+                                         const mr_tile* tiles, const int64_t* n_tiles_dev, int64_t max_tiles,
+                                         uint32_t* counter_dev, float* out, int32_t* status, void* stream) {
+    int rc = mr::check_staged_ring(ring);
+    if (rc != MR_OK) return rc;
+    if (!views || !grids || !tiles || !n_tiles_dev || !counter_dev || !out || max_tiles < 1) return MR_ERR_INVALID;
+    if ((reinterpret_cast<uintptr_t>(counter_dev) & 3) != 0) return MR_ERR_INVALID;
+    return mr::dispatch_staged(ring, views, grids, tiles, max_tiles, out, status, static_cast<cudaStream_t>(stream),
+                               n_tiles_dev, reinterpret_cast<unsigned int*>(counter_dev));
 }

@@ -17,12 +17,15 @@ def _void(x):
 
 def gaussian_taps(n, pad, sigma):
     """Even kernel g of the circular convolution that preprocess.py:21-26 applies over
-    a padded axis of length n + 2 pad: g = irfft(exp(-2 (pi f sigma)^2)), FP64,
-    truncated where it falls below 1e-20 of g[0]."""
+    a padded axis of length n + 2 pad: g = irfft(exp(-2 (pi f sigma)^2)), FP64. The
+    spectrum is cut at Nyquist, so for small sigma g has slowly decaying aliasing tails:
+    every tap above 1e-12 of g[0] is kept, up to the full circular length."""
     Np = n + 2 * pad
     f = np.fft.rfftfreq(Np)
     g = np.fft.irfft(np.exp(-2.0 * (np.pi * f * sigma) ** 2), n=Np)
-    K = min(Np // 2, int(np.ceil(10.0 * sigma)) + 1)
+    half = g[:Np // 2 + 1]
+    big = np.nonzero(np.abs(half) > 1e-12 * abs(half[0]))[0]
+    K = int(big.max()) if big.size else 0
     taps = g[:K + 1].copy()
     if 2 * K == Np:
         taps[K] *= 0.5          # m = +K and m = -K are the same circular tap: count it once
