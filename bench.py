@@ -328,6 +328,8 @@ def run_ours(args, rank, world, local):
         line["roofline_" + other[0]] = roofline(other[0], kern[other[0]], updates, args.store)
     imgs = extra.pop("_images", None)
     line.update(extra)
+    if rank == 0 and not args.no_serve:
+        line["serving"] = serving_simulation(args, dev, geom, raw_dev, flats, darks)
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"], line["accuracy"] = cpu_baseline_and_accuracy(
             args, geom, raw_dev, flats, darks, reqs, box, updates, imgs)
@@ -419,6 +421,62 @@ def bp_only_and_latency(args, dev, geom, raw_dev, flats, darks, reqs, updates, r
     }
 
 
+def serving_simulation(args, dev, geom, raw_dev, flats, darks):
+    """Live-scan serving: the scan's raw views stream into the ring at 200 views/s (groups
+    of 10) while slice requests arrive as a Poisson process at 500 req/s (sizes uniform in
+    {128, 256, 512, 1024}^2, zoom 1-8, random orientation, COR offsets within +/-10 px),
+    plus a 128^3 preview every 50 views; a continuously batched SliceServer (BF16 ring,
+    20 GB admission budget) answers them. Reports p50/p99 submit-to-host latency."""
+    import torch
+    from tomography_local_demo_b200 import SliceReconstructor
+    from tomography_local_demo_b200.server import SliceServer
+    from tomography_local_demo_b200.stream import arrival_order
+    rec = SliceReconstructor(None, geom, store="bf16", verbose=False, device=dev)
+    rec.set_flat_dark(as_u16(flats), as_u16(darks))
+    srv = SliceServer(rec, budget_bytes=20e9, max_batch=128, pool_bytes=1 << 30)
+    rng = np.random.default_rng(5)
+    V, rate, req_rate = WORKLOAD["views"], 200.0, 500.0
+    order = arrival_order(V, "interleaved")
+    futs, previews = [], []
+    # warm the server (first replay captures the graphs)
+    rec.add_raw_projections(order[:10], raw_dev[torch.from_numpy(order[:10]).to(dev)])
+    for f in [srv.submit((0, 0, 0), (0, 0, 1), n=n) for n in (128, 1024)] + [srv.submit_preview(128)]:
+        f.result()
+    rec.reset()
+    srv.latencies.clear()
+    srv.updates = 0
+    t0 = time.perf_counter()
+    next_req = t0 + rng.exponential(1.0 / req_rate)
+    sent = 0
+    while sent < V:
+        now = time.perf_counter()
+        due = int(min(V, (now - t0) * rate // 10 * 10 + 10))
+        if due > sent:
+            idx = order[sent:due]
+            rec.add_raw_projections(idx, raw_dev[torch.from_numpy(idx).to(dev)])
+            before, sent = sent, due
+            if sent // 50 > before // 50:
+                previews.append(srv.submit_preview(128))
+        while next_req <= time.perf_counter():
+            nrm = rng.normal(size=3)
+            futs.append(srv.submit(tuple(rng.uniform(-10, 10) * nrm / np.linalg.norm(nrm)), tuple(nrm),
+                                   n=int(rng.choice([128, 256, 512, 1024])), zoom=float(rng.uniform(1, 8)),
+                                   cor_shift=float(rng.uniform(-10, 10))))
+            next_req += rng.exponential(1.0 / req_rate)
+        time.sleep(0.0005)
+    for f in futs + previews:
+        f.result()
+    wall = time.perf_counter() - t0
+    srv.device_status()
+    srv.close()
+    st = srv.stats()
+    return {"requests": len(futs), "previews": len(previews), "batches": st["batches"],
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "wall_s": wall,
+            "updates_per_s": st["updates"] / wall,
+            "setup": "600 raw views at 200 views/s, Poisson 500 req/s, n in {128..1024}, zoom 1-8, "
+                     "COR +/-10 px, 128^3 preview per 50 views, bf16 ring, 20 GB budget"}
+
+
 def cpu_baseline_and_accuracy(args, geom, raw_dev, flats, darks, reqs, box, updates, imgs):
     raw = as_u16(raw_dev)
     fl, dk = as_u16(flats), as_u16(darks)
@@ -497,6 +555,7 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--store", choices=("fp32", "bf16", "fp16"), default="bf16")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / accuracy leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the live-scan serving simulation")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

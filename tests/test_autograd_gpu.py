@@ -51,27 +51,43 @@ def test_dot_product_adjoint(cuda, shift, tilt):
     assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), abs(rhs))
 
 
-def test_geometry_gradients_match_finite_differences(cuda):
+def smooth_field(A, rows, cols, n_out):
+    """Low-frequency projections and output weights. The operator is piecewise smooth
+    (bilinear taps change at pixel boundaries), so a +/-h difference straddles kinks; with
+    white-noise q and y the slope jumps there do not average out and even the exact
+    float64 autograd gradient misses the central difference by tens of percent. With
+    smooth fields the jumps are small and coherent and the two agree to ~1e-3."""
+    k = torch.arange(A, dtype=torch.float64, device="cuda")[:, None, None]
+    r = torch.arange(rows, dtype=torch.float64, device="cuda")[None, :, None]
+    c = torch.arange(cols, dtype=torch.float64, device="cuda")[None, None, :]
+    q = (torch.sin(2 * math.pi * (0.35 * r / rows + 0.45 * c / cols) + 0.7 * k)
+         + 0.5 * torch.cos(2 * math.pi * (0.6 * c / cols - 0.25 * r / rows) + 0.3 * k))
+    y = 1 + 0.5 * torch.cos(2 * math.pi * 3 * torch.arange(n_out, dtype=torch.float64, device="cuda") / n_out)
+    return q.float().contiguous(), y
+
+
+@pytest.mark.parametrize("seed", [3, 4, 5])
+def test_geometry_gradients_match_finite_differences(cuda, seed):
     """Central differences (h = 1e-2 px, 1e-3 deg) of the float64 operator against the
     analytic gradient kernel (an FP32 forward is too noisy for a 1e-3 deg step)."""
-    V, maps, box, reqs, op, q = small_case(A=12, seed=3)
-    y = torch.randn(op.n_out, device="cuda", generator=torch.Generator("cuda").manual_seed(2))
+    V, maps, box, reqs, op, _ = small_case(A=12, seed=seed)
+    q, y = smooth_field(12, 20, 28, op.n_out)
     q64 = q.double()
     grids = op.grids_at(0.0, 0.0)
 
     def L(s, t):
         f = torch64_reference(q64, maps, grids, torch.tensor(s, dtype=torch.float64, device="cuda"),
                               torch.tensor(t, dtype=torch.float64, device="cuda"), 20, 28)
-        return float((f * y.double()).sum())
+        return float((f * y).sum())
 
     for s0, t0 in ((0.4, 0.0), (-1.1, math.radians(0.3))):
-        ds, dt = op.grad_geometry(q, y, s0, t0)
+        ds, dt = op.grad_geometry(q, y.float(), s0, t0)
         h = 1e-2
         fd_s = (L(s0 + h, t0) - L(s0 - h, t0)) / (2 * h)
         ht = math.radians(1e-3)
         fd_t = (L(s0, t0 + ht) - L(s0, t0 - ht)) / (2 * ht)
-        assert abs(float(ds) - fd_s) <= 2e-2 * abs(fd_s) + 1e-6
-        assert abs(float(dt) - fd_t) <= 2e-2 * abs(fd_t) + 1e-6
+        assert abs(float(ds) - fd_s) <= 1e-2 * abs(fd_s) + 1e-6, (seed, s0, float(ds), fd_s)
+        assert abs(float(dt) - fd_t) <= 1e-2 * abs(fd_t) + 1e-6, (seed, s0, float(dt), fd_t)
 
 
 def torch64_reference(q64, maps, grids, shift, tilt, rows, cols):

@@ -225,7 +225,7 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                  int pitch, long long slot_stride, const mr_view* __restrict__ views,
                  const mr_grid* __restrict__ grids, const mr_tile* __restrict__ tiles,
                  float* __restrict__ out, int* status, const int64_t* __restrict__ n_tiles_dev,
-                 unsigned int* __restrict__ counter) {
+                 unsigned int* __restrict__ counter, long long tile_cap) {
     constexpr int W = StageGeom<T>::W;
     constexpr int S = StageGeom<T>::STAGES;
     constexpr int ESZ = (int)sizeof(T);
@@ -264,10 +264,17 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
     for (int iter = 0;; ++iter) {
         int tile_idx;
         if (counter) {
-            if (crank == 0 && tid == 0) s_next = atomicAdd(counter, 1u);
+            // rank 0 pushes the tile index into every CTA's own shared memory before the
+            // barrier; after it each CTA reads only its local copy, so no CTA touches a
+            // peer's shared memory once the cluster may start exiting (the final break)
+            if (crank == 0 && tid == 0) {
+                const unsigned int nx = atomicAdd(counter, 1u);
+                for (int r = 0; r < csize; ++r) *cluster.map_shared_rank(&s_next, r) = nx;
+            }
             cluster.sync();
-            tile_idx = (int)*cluster.map_shared_rank(&s_next, 0);
-            if ((int64_t)tile_idx >= *n_tiles_dev) break;
+            tile_idx = (int)s_next;
+            // the device count is clamped to the capacity of the tile buffer
+            if ((long long)tile_idx >= min((long long)*n_tiles_dev, tile_cap)) break;
         } else {
             if (iter > 0) break;
             tile_idx = (int)(blockIdx.x / csize);
@@ -299,6 +306,10 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
             any |= ok;
         }
         const bool tile_live = __syncthreads_or(any) != 0;
+        // warp-uniform: an 8x4 sample patch wholly outside the box is not computed
+        bool wlive[ST_PPT];
+#pragma unroll
+        for (int p = 0; p < ST_PPT; ++p) wlive[p] = __any_sync(0xffffffffu, inside[p]);
 
         if (producer && tile_live) {
             const int di_max = min(ST_TI, g.n_i - t.i0) - 1;
@@ -352,6 +363,7 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                     const uint32_t kofs = (uint32_t)MAGIC_BITS * (uint32_t)(W * ESZ + ESZ);
 #pragma unroll
                     for (int p = 0; p < ST_PPT; ++p) {
+                        if (!wlive[p]) continue;
                         const float fi = (float)(ty + 4 * p);
                         const float nu = fmaf(fi, m.cu.y, bu);
                         const float nvv = fmaf(fi, m.cv.y, bv);
@@ -385,6 +397,7 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                     const T* q = ring + (long long)(v_begin + v) * slot_stride;
 #pragma unroll
                     for (int p = 0; p < ST_PPT; ++p) {
+                        if (!wlive[p]) continue;
                         const float fi = (float)(ty + 4 * p);
                         const float nu = fmaf(fi, m.cu.y, bu);
                         const float nvv = fmaf(fi, m.cv.y, bv);
@@ -495,7 +508,7 @@ static int launch_staged(const mr_ring* ring, const mr_view* views, const mr_gri
         cfg.gridDim = dim3((unsigned)(clusters * ST_CLUSTER));
         MR_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, map, static_cast<const T*>(ring->data), ring->rows, ring->cols,
                                        ring->col_pitch, (long long)ring->slot_stride, views, grids, tiles, out,
-                                       status, n_tiles_dev, counter));
+                                       status, n_tiles_dev, counter, (long long)n_tiles));
     } else {
         const int64_t max_chunk = 2147483647LL / ST_CLUSTER;
         for (int64_t t0 = 0; t0 < n_tiles; t0 += max_chunk) {
@@ -504,7 +517,7 @@ static int launch_staged(const mr_ring* ring, const mr_view* views, const mr_gri
             MR_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, map, static_cast<const T*>(ring->data), ring->rows,
                                            ring->cols, ring->col_pitch, (long long)ring->slot_stride, views,
                                            grids, tiles + t0, out, status, (const int64_t*)nullptr,
-                                           (unsigned int*)nullptr));
+                                           (unsigned int*)nullptr, (long long)n));
         }
     }
     MR_CUDA_TRY(cudaGetLastError());
