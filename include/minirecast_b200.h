@@ -161,7 +161,8 @@ int mr_backproject_staged(const mr_ring* ring, const mr_view* views_dev,
 
 /* Persistent form of mr_backproject_staged for serving: a fixed grid of CTA clusters
  * (as many as fit on the GPU at once, at most max_tiles) pulls tile indices from a work
- * counter until it reaches *n_tiles_dev (device int64, <= max_tiles), so the launch shape
+ * counter until it reaches min(*n_tiles_dev, max_tiles) (device int64; max_tiles <= 2^31),
+ * so the launch shape
  * does not depend on the batch and the call can be captured in a CUDA graph once and
  * replayed with new grid/tile contents. counter_dev: caller-provided 4-byte device
  * scratch (4-byte aligned), zeroed on `stream` by this call; calls that share a counter

@@ -262,7 +262,7 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
     // One tile per cluster (counter == nullptr), or persistent: clusters pull tile indices
     // from the device work counter until it passes *n_tiles_dev.
     for (int iter = 0;; ++iter) {
-        int tile_idx;
+        long long tile_idx;
         if (counter) {
             // rank 0 pushes the tile index into every CTA's own shared memory before the
             // barrier; after it each CTA reads only its local copy, so no CTA touches a
@@ -272,12 +272,12 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                 for (int r = 0; r < csize; ++r) *cluster.map_shared_rank(&s_next, r) = nx;
             }
             cluster.sync();
-            tile_idx = (int)s_next;
+            tile_idx = (long long)s_next;
             // the device count is clamped to the capacity of the tile buffer
-            if ((long long)tile_idx >= min((long long)*n_tiles_dev, tile_cap)) break;
+            if (tile_idx >= min((long long)*n_tiles_dev, tile_cap)) break;
         } else {
             if (iter > 0) break;
-            tile_idx = (int)(blockIdx.x / csize);
+            tile_idx = (long long)(blockIdx.x / csize);
         }
         const mr_tile t = tiles[tile_idx];
         __syncthreads();                    // previous tile's readers of s_g are done
@@ -570,6 +570,8 @@ extern "C" int mr_backproject_persistent(const mr_ring* ring, const mr_view* vie
     int rc = mr::check_staged_ring(ring);
     if (rc != MR_OK) return rc;
     if (!views || !grids || !tiles || !n_tiles_dev || !counter_dev || !out || max_tiles < 1) return MR_ERR_INVALID;
+    // the 32-bit work counter must not wrap while the last clusters overshoot the count
+    if (max_tiles > (int64_t(1) << 31)) return MR_ERR_INVALID;
     if ((reinterpret_cast<uintptr_t>(counter_dev) & 3) != 0) return MR_ERR_INVALID;
     return mr::dispatch_staged(ring, views, grids, tiles, max_tiles, out, status, static_cast<cudaStream_t>(stream),
                                n_tiles_dev, reinterpret_cast<unsigned int*>(counter_dev));
