@@ -34,6 +34,8 @@ extern "C" {
 #define MR_ERR_CUDA         -2   /* a CUDA runtime call or launch failed */
 #define MR_ERR_UNSUPPORTED  -3   /* valid but not built (e.g. FFT length out of range) */
 #define MR_ERR_TIMEOUT      -4   /* a bounded device-side wait gave up */
+#define MR_ERR_SCRATCH_LIMIT -5  /* the request needs more than the library's fixed device
+                                    scratch (mr_backproject_persistent_noalloc) */
 
 /* ---- element types ------------------------------------------------------------- */
 #define MR_F32   0
@@ -172,6 +174,30 @@ int mr_backproject_persistent(const mr_ring* ring, const mr_view* views_dev,
                               const int64_t* n_tiles_dev, int64_t max_tiles,
                               uint32_t* counter_dev, float* out_dev, int32_t* status_dev,
                               void* stream);
+
+/* No counterpart in the reference (minirecast runs on the CPU and never allocates device
+ * memory). The same back-projection as mr_backproject_persistent, for callers that cannot
+ * call cudaMalloc: a host whose device memory is handed out by another component (an
+ * acquisition or frame-grabber SDK, an application-wide memory pool) and that therefore
+ * owns no device buffer of its own to use as the work counter, or code on a live
+ * acquisition path where an allocation could synchronise the device and stall the scan.
+ * The work counter lives in the library's own device scratch: a 256-byte static array
+ * (MR_NOALLOC_SCRATCH_BYTES) that every GPU which loads the library holds until the
+ * process exits. Nothing is allocated by this call; the caller still passes every input
+ * and output. The counter is zeroed on `stream` by each call.
+ *   - The device that owns `stream` must be the current device.
+ *   - The first call on a device looks up the array's device address (and may load the
+ *     library's device code); make that first call before any stream capture.
+ *   - Every call on a device shares the one counter: calls that overlap on the GPU race
+ *     and give wrong results. Order them on one stream (or wait between them).
+ *   - max_tiles above MR_NOALLOC_MAX_TILES (the range one 32-bit counter can hand out)
+ *     returns MR_ERR_SCRATCH_LIMIT before anything is launched. */
+#define MR_NOALLOC_SCRATCH_BYTES 256
+#define MR_NOALLOC_MAX_TILES (((int64_t)1) << 31)
+int mr_backproject_persistent_noalloc(const mr_ring* ring, const mr_view* views_dev,
+                                      const mr_grid* grids_dev, const mr_tile* tiles_dev,
+                                      const int64_t* n_tiles_dev, int64_t max_tiles,
+                                      float* out_dev, int32_t* status_dev, void* stream);
 
 /* ---- derivatives of the back-projection (no counterpart in minirecast: the reference
  * back-projector is not differentiable; the forward operator is recon.py:156-219) ----

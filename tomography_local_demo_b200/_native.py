@@ -16,6 +16,8 @@ MR_ERR_INVALID = -1
 MR_ERR_CUDA = -2
 MR_ERR_UNSUPPORTED = -3
 MR_ERR_TIMEOUT = -4
+MR_ERR_SCRATCH_LIMIT = -5
+MR_NOALLOC_MAX_TILES = 1 << 31
 
 MR_F32, MR_BF16, MR_F16, MR_U16 = 0, 1, 2, 3
 MR_PARALLEL, MR_CONE = 0, 1
@@ -56,6 +58,7 @@ SIGNATURES = {
     "mr_backproject": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P]),
     "mr_backproject_staged": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P, _P]),
     "mr_backproject_persistent": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _P, _I64, _P, _P, _P, _P]),
+    "mr_backproject_persistent_noalloc": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _P, _I64, _P, _P, _P]),
     "mr_backproject_matched": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P]),
     "mr_project_adjoint": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P]),
     "mr_bp_grad_geom": (ctypes.c_int, [ctypes.POINTER(MrRing), _P, _P, _P, _I64, _P, _P, _P]),

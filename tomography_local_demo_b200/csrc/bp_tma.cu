@@ -576,3 +576,55 @@ extern "C" int mr_backproject_persistent(const mr_ring* ring, const mr_view* vie
     return mr::dispatch_staged(ring, views, grids, tiles, max_tiles, out, status, static_cast<cudaStream_t>(stream),
                                n_tiles_dev, reinterpret_cast<unsigned int*>(counter_dev));
 }
+
+// ---------------------------------------------------------------- no-allocation variant
+// The persistent launch needs one 32-bit work counter in device memory. Callers that
+// cannot allocate device memory get it from this file-scope array instead; every GPU that
+// loads the library holds it until the process exits, and every call shares it.
+static __device__ __align__(256) unsigned int g_noalloc_scratch[MR_NOALLOC_SCRATCH_BYTES / 4];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned int* g_noalloc_addr[kNoallocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device.
+// In host code the array's name is only a host-side stand-in, never a device address.
+int noalloc_counter(cudaStream_t stream, unsigned int** counter) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return MR_ERR_CUDA;
+    if (dev >= kNoallocMaxDevices) return MR_ERR_UNSUPPORTED;
+    if (stream) {
+        int sdev = -1;
+        if (cudaStreamGetDevice(stream, &sdev) != cudaSuccess) return MR_ERR_CUDA;
+        if (sdev != dev) return MR_ERR_INVALID;      // the stream's device must be current
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return MR_ERR_CUDA;
+        }
+        g_noalloc_addr[dev] = static_cast<unsigned int*>(p);
+    }
+    *counter = g_noalloc_addr[dev];
+    return MR_OK;
+}
+}  // namespace
+
+extern "C" int mr_backproject_persistent_noalloc(const mr_ring* ring, const mr_view* views,
+                                                 const mr_grid* grids, const mr_tile* tiles,
+                                                 const int64_t* n_tiles_dev, int64_t max_tiles, float* out,
+                                                 int32_t* status, void* stream) {
+    int rc = mr::check_staged_ring(ring);
+    if (rc != MR_OK) return rc;
+    if (!views || !grids || !tiles || !n_tiles_dev || !out || max_tiles < 1) return MR_ERR_INVALID;
+    if (max_tiles > MR_NOALLOC_MAX_TILES) return MR_ERR_SCRATCH_LIMIT;
+    unsigned int* counter = nullptr;
+    rc = noalloc_counter(static_cast<cudaStream_t>(stream), &counter);
+    if (rc != MR_OK) return rc;
+    // the shared launch path zeroes the counter on `stream` before the kernel
+    return mr::dispatch_staged(ring, views, grids, tiles, max_tiles, out, status, static_cast<cudaStream_t>(stream),
+                               n_tiles_dev, counter);
+}

@@ -10,6 +10,7 @@ extern "C" const char* mr_status_string(int status) {
         case MR_ERR_CUDA: return "CUDA runtime or launch error";
         case MR_ERR_UNSUPPORTED: return "unsupported configuration";
         case MR_ERR_TIMEOUT: return "device-side wait timed out";
+        case MR_ERR_SCRATCH_LIMIT: return "request exceeds the fixed device scratch of the no-allocation entry point";
         default: return "unknown status";
     }
 }
