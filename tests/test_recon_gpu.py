@@ -194,3 +194,39 @@ def test_errors_match_reference(cuda):
     assert rec.reconstruct_points(np.zeros((5, 3))).tolist() == [0.0] * 5
     img, _ = rec.reconstruct_plane((0, 0, 0), (0, 0, 1), n=16)
     assert np.all(img == 0)
+
+
+@pytest.mark.parametrize("kind", ["cuda", "pinned", "numpy", "pageable"])
+def test_raw_ingest_input_kinds_and_chunked_upload(cuda, kind):
+    """add_raw_projections from device counts (one launch) and from host counts (uploaded
+    in chunks that overlap the filtering, staged through pinned buffers when pageable):
+    every path stores the same ring bit for bit, also when the call repeats views
+    (dedup) and when the chunks outnumber the pinned staging buffers."""
+    import torch
+    geom = circular_cone_vectors(40, 300.0, 600.0, 24, 36, 3.0)
+    rng = np.random.default_rng(4)
+    raw = rng.integers(2000, 45000, (40, 48, 72)).astype(np.uint16)        # binned 2x2 on ingest
+    flat = rng.normal(50000, 500, (2, 48, 72)).clip(0, 65535).astype(np.uint16)
+    dark = rng.normal(100, 5, (2, 48, 72)).clip(0, 65535).astype(np.uint16)
+
+    def ingest(src, chunk_bytes):
+        rec = SliceReconstructor(None, geom, verbose=False, store="bf16")
+        rec.set_flat_dark(flat, dark, bin=2, flip_rows=True)
+        rec.upload_chunk_bytes = chunk_bytes
+        order = arrival_order(40, "interleaved")
+        rec.add_raw_projections(order[:25], src(order[:25]))
+        rec.add_raw_projections(order[20:], src(order[20:]))          # 5 repeated views
+        torch.cuda.synchronize()
+        assert rec.n == 40
+        return rec, rec._ring.float().cpu().numpy(), rec._order.copy()
+
+    want_rec, want, want_order = ingest(lambda i: torch.from_numpy(raw[i].view(np.int16)).cuda(), 1 << 30)
+    src = {"cuda": lambda i: torch.from_numpy(raw[i].view(np.int16)).cuda(),
+           "pinned": lambda i: torch.from_numpy(raw[i].view(np.int16)).pin_memory(),
+           "numpy": lambda i: raw[i],
+           "pageable": lambda i: torch.from_numpy(raw[i].view(np.int16).copy())}[kind]
+    rec, got, order = ingest(src, 3 * 48 * 72 * 2)                         # 3 views per chunk
+    np.testing.assert_array_equal(order, want_order)
+    np.testing.assert_array_equal(got, want)
+    req = dict(origin=(1.0, -2.0, 0.5), normal=(0.3, 0.2, 1.0), n=40)
+    np.testing.assert_array_equal(rec.reconstruct_planes([req])[0], want_rec.reconstruct_planes([req])[0])

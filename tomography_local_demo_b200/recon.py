@@ -492,6 +492,7 @@ class SliceReconstructor:
         with torch.cuda.device(self.device):
             self.stream = torch.cuda.Stream(self.device)          # reconstruction
             self.ingest_stream = torch.cuda.Stream(self.device)   # filtering of new views
+            self.copy_stream = torch.cuda.Stream(self.device)     # host -> device raw counts
             self._tables = _FilterTables(C, window, self.device)
             self._ring = torch.zeros((self.n_total, R, self._pitch), dtype=tdtype, device=self.device)
             self._views_host = np.zeros(self.n_total, dtype=N.VIEW_DTYPE)
@@ -499,6 +500,9 @@ class SliceReconstructor:
                                           device=self.device)
         self._ring_c = _ring_struct(self._ring, self._dtype_code, self._kind_code, R, C)
         self._ingest_event = None
+        self._raw_dev = None            # device staging of host raw counts (grows on demand)
+        self._raw_pinned = []           # pinned staging of pageable raw counts, one per chunk slot
+        self.upload_chunk_bytes = 16 << 20   # raw bytes per overlapped upload + ingest chunk
         self.kernel_timer = None        # a KernelTimer records launch durations when set
         self.bp_kernel = "staged"       # "plain": direct-gather kernel for every request
         with torch.cuda.device(self.device):
@@ -532,7 +536,10 @@ class SliceReconstructor:
             rec = self._views_host[n0:n1].view(np.uint8)
             with torch.cuda.stream(self.ingest_stream):
                 dst = self._views_dev[n0 * N.VIEW_DTYPE.itemsize:n1 * N.VIEW_DTYPE.itemsize]
-                dst.copy_(torch.from_numpy(rec.copy()), non_blocking=False)
+                # pinned source: the copy is asynchronous and the host does not wait for the
+                # ingest kernels queued before it (the caching host allocator keeps the
+                # buffer alive until the copy has run)
+                dst.copy_(torch.from_numpy(rec.copy()).pin_memory(), non_blocking=True)
             event.record(self.ingest_stream)
             self._ingest_event = event
             self.n = n1
@@ -613,8 +620,10 @@ class SliceReconstructor:
 
     def add_raw_projections(self, indices, raw):
         """Fused ingest of raw detector counts: raw [k, R0, C0] uint16 (NumPy, pinned or
-        CUDA tensor) -> bin, (P-D)*gain, clip 1e-3, -log, FDK weight, ramp filter, store;
-        one kernel launch (mr_ingest_u16). Needs set_flat_dark() first."""
+        CUDA tensor) -> bin, (P-D)*gain, clip 1e-3, -log, FDK weight, ramp filter, store
+        (mr_ingest_u16). A CUDA tensor is filtered in one launch; host counts are uploaded
+        in chunks whose transfers overlap the filtering of the previous chunk. Needs
+        set_flat_dark() first."""
         if getattr(self, "_gain", None) is None:
             raise RuntimeError("call set_flat_dark() before add_raw_projections()")
         if self.gaussian or self.tilt:
@@ -638,31 +647,92 @@ class SliceReconstructor:
             k = len(indices)
             n0 = self.n
             slots = np.arange(n0, n0 + k)
+            fv_host = self._filter_views(indices, slots)
+            on_device = isinstance(raw, torch.Tensor) and raw.is_cuda
             with torch.cuda.device(self.device), torch.cuda.stream(self.ingest_stream):
-                if isinstance(raw, torch.Tensor):
+                fv_pinned = torch.from_numpy(np.ascontiguousarray(fv_host).view(np.uint8).copy()).pin_memory()
+                fv = fv_pinned.to(self.device, non_blocking=True)
+                if on_device:
                     x = raw.view(torch.int16) if raw.dtype == torch.uint16 else raw
                     x = x.to(self.device, non_blocking=True).contiguous()
+                    if x.element_size() != 2:
+                        raise ValueError("raw counts must be 16-bit")
+                    self._ingest_launch(x, 0, k, fv)
+                    x.record_stream(self.ingest_stream)
                 else:
-                    x = torch.from_numpy(np.ascontiguousarray(raw, dtype=np.uint16).view(np.int16))
-                    x = x.to(self.device, non_blocking=True)
-                if x.element_size() != 2:
-                    raise ValueError("raw counts must be 16-bit")
-                fv = _struct_tensor(self._filter_views(indices, slots), self.device)
-                lib = N.load()
-                t = self._tables
-                tm = self.kernel_timer
-                ev0 = tm.start(self.ingest_stream) if tm is not None else None
-                st = lib.mr_ingest_u16(ctypes_void(x.data_ptr()), x.shape[1] * x.shape[2], x.shape[2], b,
-                                       int(self._raw_flip), ctypes_void(self._dark.data_ptr()),
-                                       ctypes_void(self._gain.data_ptr()), k, ctypes_void(fv.data_ptr()),
-                                       ctypes_void(t.H.data_ptr()), ctypes_void(t.tw.data_ptr()), t.log2n,
-                                       self._ring_c, ctypes_void(self.ingest_stream.cuda_stream))
-                if tm is not None:
-                    tm.stop("mr_ingest_u16", ev0, self.ingest_stream)
-                N.check(st, "mr_ingest_u16")
-                x.record_stream(self.ingest_stream)
+                    self._ingest_host(raw, k, fv)
                 ev = torch.cuda.Event()
             return self._admit(indices, slots, ev)
+
+    def _ingest_launch(self, x, c0, c1, fv):
+        """mr_ingest_u16 of views [c0, c1) of the device raw block x on the ingest stream."""
+        lib = N.load()
+        t = self._tables
+        tm = self.kernel_timer
+        ev0 = tm.start(self.ingest_stream) if tm is not None else None
+        view_bytes = x.shape[1] * x.shape[2] * 2
+        st = lib.mr_ingest_u16(ctypes_void(x.data_ptr() + c0 * view_bytes), x.shape[1] * x.shape[2], x.shape[2],
+                               self._raw_bin, int(self._raw_flip), ctypes_void(self._dark.data_ptr()),
+                               ctypes_void(self._gain.data_ptr()), c1 - c0,
+                               ctypes_void(fv.data_ptr() + c0 * N.FILTER_VIEW_DTYPE.itemsize),
+                               ctypes_void(t.H.data_ptr()), ctypes_void(t.tw.data_ptr()), t.log2n,
+                               self._ring_c, ctypes_void(self.ingest_stream.cuda_stream))
+        if tm is not None:
+            tm.stop("mr_ingest_u16", ev0, self.ingest_stream)
+        N.check(st, "mr_ingest_u16")
+
+    def _ingest_host(self, raw, k, fv):
+        """Upload host raw counts in chunks on the copy stream and filter each chunk on the
+        ingest stream as soon as it has landed, so the PCIe transfer of chunk i+1 overlaps
+        the ingest of chunk i. Pinned torch tensors are copied directly; anything else
+        (NumPy, pageable tensors) is staged through reusable pinned buffers."""
+        if isinstance(raw, torch.Tensor):
+            if raw.element_size() != 2:
+                raise ValueError("raw counts must be 16-bit")
+            host = raw.view(torch.int16) if raw.dtype == torch.uint16 else raw
+            host = host.contiguous()
+            pinned = host.is_pinned()
+            host_np = None if pinned else host.numpy()
+        else:
+            arr = np.asarray(raw)
+            if arr.dtype.itemsize != 2:
+                raise ValueError("raw counts must be 16-bit")
+            host_np = np.ascontiguousarray(arr).view(np.int16)
+            host, pinned = None, False
+        shape = tuple(host.shape if host is not None else host_np.shape)
+        view_bytes = shape[1] * shape[2] * 2
+        chunk = max(1, min(k, self.upload_chunk_bytes // view_bytes))
+        need = k * shape[1] * shape[2]
+        if self._raw_dev is None or self._raw_dev.numel() < need:
+            self._raw_dev = torch.empty(need, dtype=torch.int16, device=self.device)
+        x = self._raw_dev[:need].view(k, shape[1], shape[2])
+        # the previous call's ingest kernels must be done reading the staging buffer
+        self.copy_stream.wait_stream(self.ingest_stream)
+        if not pinned:
+            n_slots = 3
+            while len(self._raw_pinned) < n_slots:
+                self._raw_pinned.append([None, None])        # [pinned tensor, event of its last copy]
+        for i, c0 in enumerate(range(0, k, chunk)):
+            c1 = min(k, c0 + chunk)
+            with torch.cuda.stream(self.copy_stream):
+                if pinned:
+                    x[c0:c1].copy_(host[c0:c1], non_blocking=True)
+                else:
+                    slot = self._raw_pinned[i % len(self._raw_pinned)]
+                    n_el = (c1 - c0) * shape[1] * shape[2]
+                    if slot[0] is None or slot[0].numel() < chunk * shape[1] * shape[2]:
+                        slot[0] = torch.empty(chunk * shape[1] * shape[2], dtype=torch.int16).pin_memory()
+                    elif slot[1] is not None:
+                        slot[1].synchronize()                # its previous copy has left the buffer
+                    buf = slot[0][:n_el]
+                    np.copyto(buf.numpy(), host_np[c0:c1].reshape(-1))
+                    x[c0:c1].copy_(buf.view(c1 - c0, shape[1], shape[2]), non_blocking=True)
+                    slot[1] = torch.cuda.Event()
+                    slot[1].record(self.copy_stream)
+                landed = torch.cuda.Event()
+                landed.record(self.copy_stream)
+            self.ingest_stream.wait_event(landed)
+            self._ingest_launch(x, c0, c1, fv)
 
     # ----------------------------------------------------------- info
     @property
