@@ -248,6 +248,40 @@ int mr_ingest_u16(const uint16_t* raw, int64_t s_view, int64_t s_row,
                   const float* H_dev, const float* twiddle_dev, int32_t log2n,
                   const mr_ring* ring, void* stream);
 
+/* ---- tensor-core Toeplitz filter (the measured alternative to the FFT filter) ------
+ * Same contracts as mr_filter_f32 / mr_ingest_u16 (recon.py:58-104; flexray.py:174-184 +
+ * hdf5.py:73-78 for the raw correction), with the row filter computed as a GEMM on the
+ * tcgen05 tensor cores: for outputs and inputs inside a row, filtering is y = T x with
+ * the Toeplitz matrix T[n][j] = g[(n - j) mod n_fft], g = ifft(H) for tau = 1.
+ * Operands are split into two 16-bit parts (x = x_hi + x_lo, g = g_hi + g_lo; `format`
+ * MR_F16 or MR_BF16) with FP32 accumulation; the hi/lo cross terms are kept on the three
+ * 64-wide block diagonals nearest the main one, where |g| is large. FP16 parts carry 22
+ * bits (filtered rows within ~1e-5 of FP64), BF16 parts 16 bits (~5e-4: the ramp filter
+ * cancels ~400x on smooth rows). FP16 operands are brought into range by powers of two:
+ * `t_scale` (from mr_toeplitz_image) for g, `x_scale` for the inputs (the FP32 entry
+ * point needs max |x| * x_scale < 2^14; the raw entry point uses 1024, since
+ * |-log(max(t, 1e-3))| < 11.1).
+ * Rows of at most 512 columns (MR_ERR_UNSUPPORTED beyond); col_pitch and slot_stride
+ * multiples of 8 elements, 16-byte aligned ring.
+ * `image_dev`: device copy of the operand built by mr_toeplitz_image (16-byte aligned).
+ * `status_dev` (may be NULL) receives MR_ERR_TIMEOUT if a bounded device wait gave up. */
+int64_t mr_toeplitz_image_bytes(int32_t cols);
+/* Host-only: write the split Toeplitz blocks of the FP64 kernel g[0..n_fft) in `format`
+ * into `image_host` (mr_toeplitz_image_bytes(cols) bytes), in the kernel's shared-memory
+ * layout (SWIZZLE_128B K-major), and the power-of-two scale applied to g in *t_scale. */
+int mr_toeplitz_image(const double* g, int32_t n_fft, int32_t cols, int32_t format,
+                      void* image_host, float* t_scale);
+int mr_filter_f32_tc(const float* block, int64_t s_view, int64_t s_row, int32_t k,
+                     const mr_filter_view* views_dev, const void* image_dev, int32_t format,
+                     float t_scale, float x_scale, int32_t n_fft,
+                     const mr_ring* ring, int32_t* status_dev, void* stream);
+int mr_ingest_u16_tc(const uint16_t* raw, int64_t s_view, int64_t s_row,
+                     int32_t bin, int32_t flip_rows,
+                     const float* dark_dev, const float* gain_dev,
+                     int32_t k, const mr_filter_view* views_dev,
+                     const void* image_dev, int32_t format, float t_scale, int32_t n_fft,
+                     const mr_ring* ring, int32_t* status_dev, void* stream);
+
 /* ---- rotation-centre search score ---------------------------------------------
  * Replaces the scoring loop of recon.py:498-519 (estimate_cor): for each of n_imgs
  * images (f32, device, image i at imgs + i*stride, n_pix pixels) the FP64 score

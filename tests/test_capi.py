@@ -25,7 +25,7 @@ def declared_functions():
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        names += re.findall(r"^\s*(?:int|void|const\s+char\s*\*)\s*(mr_\w+)\s*\(", text, flags=re.M)
+        names += re.findall(r"^\s*(?:int|int64_t|void|const\s+char\s*\*)\s*(mr_\w+)\s*\(", text, flags=re.M)
     return sorted(set(names))
 
 

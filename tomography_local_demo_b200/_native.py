@@ -66,6 +66,12 @@ SIGNATURES = {
                                      ctypes.POINTER(MrRing), _P]),
     "mr_ingest_u16": (ctypes.c_int, [_P, _I64, _I64, _I32, _I32, _P, _P, _I32, _P, _P, _P, _I32,
                                      ctypes.POINTER(MrRing), _P]),
+    "mr_toeplitz_image_bytes": (ctypes.c_int64, [_I32]),
+    "mr_toeplitz_image": (ctypes.c_int, [_P, _I32, _I32, _I32, _P, ctypes.POINTER(ctypes.c_float)]),
+    "mr_filter_f32_tc": (ctypes.c_int, [_P, _I64, _I64, _I32, _P, _P, _I32, ctypes.c_float, ctypes.c_float, _I32,
+                                        ctypes.POINTER(MrRing), _P, _P]),
+    "mr_ingest_u16_tc": (ctypes.c_int, [_P, _I64, _I64, _I32, _I32, _P, _P, _I32, _P, _P, _I32, ctypes.c_float,
+                                        _I32, ctypes.POINTER(MrRing), _P, _P]),
     "mr_slice_entropy": (ctypes.c_int, [_P, _I32, _I64, _I32, _I32, _P, _P]),
     "mr_rotate_f32": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, ctypes.c_double, _P]),
     "mr_gaussian_axis_f32": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _I32, _I32, _P, _I32, _P]),

@@ -1,0 +1,653 @@
+// Ramp / FDK row filter as a Toeplitz GEMM on the 5th-generation tensor cores (tcgen05).
+//
+// The reference filters each detector row by zero padding to N = 2^ceil(log2(2C)),
+// multiplying its spectrum by the window response H and transforming back
+// (minirecast recon.py:34-64, 85-104). For outputs and inputs inside the row that is the
+// linear map y = T x with T[n][j] = g[(n - j) mod N], g = ifft(H) - a C x C Toeplitz
+// matrix - so filtering a stack of rows is one dense GEMM  Y[rows, C] = X[rows, C] T^T.
+//
+// Layout of the contraction (one 128-row tile of detector rows per pass):
+//   * K and N are cut into 64-wide blocks; block (J, I) of T depends only on d = J - I,
+//     so the whole operand is 2*KB - 1 distinct 64 x 64 blocks (KB = ceil(C / 64) <= 8).
+//     They stay resident in shared memory for the CTA's lifetime (<= 120 KB).
+//   * split 16-bit operands: x = x_hi + x_lo and g = g_hi + g_lo, each part rounded to
+//     FP16 (default) or BF16; the tensor cores accumulate x_hi g_hi everywhere plus
+//     x_hi g_lo + x_lo g_hi on the three block diagonals |d| <= 1, where |g| is large (the
+//     ramp kernel decays as 1/k^2). The ramp filter cancels strongly on smooth rows (output
+//     norm ~1/400 of the input's), so the operand precision matters: FP16 hi+lo carries 22
+//     bits (~1e-5 relative error of the filtered row), BF16 hi+lo 16 bits (~5e-4). FP16
+//     operands are scaled by powers of two into range: g by `t_scale` (max |g| t_scale in
+//     [2^13, 2^14)), the inputs by `x_scale`; the epilogue divides both out.
+//   * producer warps read the inputs (raw uint16 counts with flat/dark correction and
+//     -log, or FP32 rows), apply the FDK cosine weight, split them and write them into a
+//     2-stage ring of SWIZZLE_128B K-major tiles; one thread issues tcgen05.mma (M = 128,
+//     N <= 256, K = 16) into an FP32 accumulator of KB * 64 columns in tensor memory; four
+//     epilogue warps read it back with tcgen05.ld, scale by the view's gain and store into
+//     the filtered-view ring (FP32 / BF16 / FP16).
+//   * every mbarrier wait is bounded in time; a wait that gives up sets an abort flag in
+//     shared memory that ends every role, drains the issued MMAs and frees tensor memory.
+#include "mr_common.cuh"
+
+#include <math.h>
+#include <string.h>
+
+namespace mr {
+namespace tc {
+
+constexpr int TILE_M = 128;
+constexpr int KB_MAX = 8;                       // C <= 512
+constexpr int EPI_WARPS = 4;                    // warps 0..3 (TMEM lane quarters)
+constexpr int MMA_WARP = 4;
+constexpr int PROD_WARPS = 8;                   // warps 5..12
+constexpr int THREADS = 32 * (EPI_WARPS + 1 + PROD_WARPS);
+constexpr int BLOCK_BYTES = 64 * 64 * 2;        // one 64 x 64 block of 16-bit values (8 KB)
+constexpr int A_TILE_BYTES = TILE_M * 128;      // 128 rows x 64 values (16 KB)
+constexpr int STAGES = 2;
+constexpr int STAGE_BYTES = 2 * A_TILE_BYTES;   // hi + lo
+constexpr unsigned long long WAIT_NS = 2000000000ull;
+
+struct RowInfo {                                // one GEMM row (detector row of a view)
+    const void* src;                            // first input element of the row
+    int pix;                                    // r * C (offset into dark / gain), -1 = padding row
+    float b;                                    // FDK row term b0 + r db
+    float a0, da, sdd;
+    int pad;
+};
+
+struct Args {
+    const void* src;                            // uint16 raw counts or FP32 rows
+    long long s_view, s_row;
+    int bin, flip;
+    const float* dark;
+    const float* gain;
+    const mr_filter_view* views;
+    const unsigned char* bimg;                  // split Toeplitz blocks, shared-memory image
+    float x_scale;                              // inputs are multiplied by this before the split
+    float out_mul;                              // n_fft / (x_scale * t_scale)
+    void* ring;
+    int dtype, rows, cols, pitch, n_slots;
+    long long slot_stride;
+    long long m_total;                          // k * rows
+    int kb;
+    int vec_src, vec_fld;                       // 4-byte raw pairs / 8-byte float pairs usable
+    int* status;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void bar_init(uint64_t* b, uint32_t n) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(n));
+}
+__device__ __forceinline__ void bar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
+}
+__device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait: false if another role aborted or this wait exceeded WAIT_NS (then it
+// raises the abort flag and reports MR_ERR_TIMEOUT).
+__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag, int* status) {
+    const unsigned long long t0 = global_ns();
+    for (uint32_t it = 0;; ++it) {
+        if (bar_try(b, parity)) return true;
+        if ((it & 63u) == 63u) {
+            if (*abort_flag) return false;
+            if (global_ns() - t0 > WAIT_NS) {
+                *abort_flag = 1;
+                if (status) atomicExch(status, MR_ERR_TIMEOUT);
+                return false;
+            }
+        }
+    }
+}
+
+// Shared-memory matrix descriptor: K-major, SWIZZLE_128B (rows of 128 bytes, 8-row atoms
+// of 1024 bytes), stride between atoms 1024 bytes, descriptor version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+// Instruction descriptor of kind::f16: F16 x F16 (or BF16 x BF16) -> F32, both K-major, M = 128.
+template <bool F16>
+__device__ __forceinline__ uint32_t idesc(int n) {
+    constexpr uint32_t fmt = F16 ? 0u : 1u;
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TILE_M >> 4) << 24);
+}
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(id), "r"(accumulate));
+}
+__device__ __forceinline__ void mma_commit(uint64_t* b) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_addr(b))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    // load and wait in one statement: the outputs are defined only once the load is complete
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int e = 0; e < 16; ++e) v[e] = __uint_as_float(r[e]);
+}
+
+// Byte offset of element (row, k) (k even: a pair of 16-bit values) in a SWIZZLE_128B
+// K-major tile: 16-byte chunk index XOR (row mod 8) inside each 128-byte row.
+__device__ __forceinline__ uint32_t swz(int row, int k) {
+    return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((((k >> 3) ^ (row & 7)) & 7) << 4) + (k & 7) * 2);
+}
+
+// x -> (hi, lo) 16-bit parts, two columns packed per 32-bit word.
+template <bool F16>
+__device__ __forceinline__ void split2(float2 x, uint32_t& hi, uint32_t& lo) {
+    if (F16) {
+        x.x = fminf(fmaxf(x.x, -65504.f), 65504.f);     // finite even for out-of-range inputs
+        x.y = fminf(fmaxf(x.y, -65504.f), 65504.f);
+        const __half2 h = __floats2half2_rn(x.x, x.y);
+        const float2 hf = __half22float2(h);
+        const __half2 l = __floats2half2_rn(x.x - hf.x, x.y - hf.y);
+        hi = *reinterpret_cast<const uint32_t*>(&h);
+        lo = *reinterpret_cast<const uint32_t*>(&l);
+    } else {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(x.x, x.y);
+        const float2 hf = __bfloat1622float2(h);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(x.x - hf.x, x.y - hf.y);
+        hi = *reinterpret_cast<const uint32_t*>(&h);
+        lo = *reinterpret_cast<const uint32_t*>(&l);
+    }
+}
+
+template <bool RAW>
+__device__ __forceinline__ float2 load_pair(const Args& A, const RowInfo& ri, int c) {
+    // columns c, c + 1 of the row (c + 1 past the row reads as 0)
+    const bool two = c + 1 < A.cols;
+    float2 s;
+    if (RAW) {
+        const uint16_t* p = static_cast<const uint16_t*>(ri.src);
+        if (A.bin == 1) {
+            if (A.vec_src && two) {
+                const uint32_t w = __ldg(reinterpret_cast<const unsigned int*>(p + c));
+                s = make_float2((float)(w & 0xFFFFu), (float)(w >> 16));
+            } else {
+                s = make_float2((float)__ldg(p + c), two ? (float)__ldg(p + c + 1) : 0.f);
+            }
+        } else {
+            const int b = A.bin;
+            float acc[2] = {0.f, 0.f};
+            for (int e = 0; e < (two ? 2 : 1); ++e) {
+                const uint16_t* q = p + (long long)(c + e) * b;
+                for (int dy = 0; dy < b; ++dy)
+                    for (int dx = 0; dx < b; ++dx) acc[e] += (float)__ldg(q + (long long)dy * A.s_row + dx);
+                acc[e] = __fdiv_rn(acc[e], (float)(b * b));
+            }
+            s = make_float2(acc[0], acc[1]);
+        }
+        float2 dk, gn;
+        const int pix = ri.pix + c;
+        if (A.vec_fld && two) {
+            dk = __ldg(reinterpret_cast<const float2*>(A.dark + pix));
+            gn = __ldg(reinterpret_cast<const float2*>(A.gain + pix));
+        } else {
+            dk = make_float2(__ldg(A.dark + pix), two ? __ldg(A.dark + pix + 1) : 0.f);
+            gn = make_float2(__ldg(A.gain + pix), two ? __ldg(A.gain + pix + 1) : 0.f);
+        }
+        s.x = -__logf(fmaxf((s.x - dk.x) * gn.x, 1e-3f));
+        s.y = two ? -__logf(fmaxf((s.y - dk.y) * gn.y, 1e-3f)) : 0.f;
+    } else {
+        const float* p = static_cast<const float*>(ri.src);
+        if (A.vec_src && two) {
+            s = __ldg(reinterpret_cast<const float2*>(p + c));
+        } else {
+            s = make_float2(__ldg(p + c), two ? __ldg(p + c + 1) : 0.f);
+        }
+    }
+    if (ri.sdd != 0.f) {                        // FDK cosine weight, same arithmetic as the FFT path
+        const float a1 = fmaf((float)c, ri.da, ri.a0), a2 = fmaf((float)(c + 1), ri.da, ri.a0);
+        s.x *= ri.sdd * rsqrtf(fmaf(ri.b, ri.b, fmaf(ri.sdd, ri.sdd, a1 * a1)));
+        s.y *= ri.sdd * rsqrtf(fmaf(ri.b, ri.b, fmaf(ri.sdd, ri.sdd, a2 * a2)));
+    }
+    return s;
+}
+
+template <bool RAW, bool F16>
+__global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* sm = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    const int KB = A.kb;
+    const int NCOL = KB * 64;
+    const int hi_blocks = 2 * KB - 1;
+    unsigned char* b_hi = sm;
+    unsigned char* b_lo = b_hi + hi_blocks * BLOCK_BYTES;              // d = -1, 0, 1
+    unsigned char* a_st = b_lo + 3 * BLOCK_BYTES;                      // STAGES x (hi, lo)
+    RowInfo* rows = reinterpret_cast<RowInfo*>(a_st + STAGES * STAGE_BYTES);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(rows + TILE_M);
+    uint64_t* full = bars;                      // [STAGES], one arrival per producer warp
+    uint64_t* empty = bars + STAGES;            // [STAGES], tcgen05.commit
+    uint64_t* tfull = bars + 2 * STAGES;        // accumulator ready
+    uint64_t* tempty = tfull + 1;               // accumulator drained (one arrival per epilogue warp)
+    uint64_t* drain = tfull + 2;                // every issued MMA has completed
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(drain + 1);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1) + 1;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // resident operand: the split Toeplitz blocks, copied once (16-byte vectors)
+    {
+        const int nbytes = (hi_blocks + 3) * BLOCK_BYTES;
+        const uint4* src = reinterpret_cast<const uint4*>(A.bimg);
+        uint4* dst = reinterpret_cast<uint4*>(b_hi);
+        for (int i = tid; i < nbytes / 16; i += THREADS) dst[i] = __ldg(src + i);
+        fence_async_smem();
+    }
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            bar_init(&full[s], PROD_WARPS);
+            bar_init(&empty[s], 1);
+        }
+        bar_init(tfull, 1);
+        bar_init(tempty, EPI_WARPS);
+        bar_init(drain, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    const uint32_t tmem_cols = NCOL <= 64 ? 64 : (NCOL <= 128 ? 128 : (NCOL <= 256 ? 256 : 512));
+    if (warp == MMA_WARP) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const long long n_tiles = (A.m_total + TILE_M - 1) / TILE_M;
+
+    if (warp >= MMA_WARP + 1) {
+        // ---------------- producers: inputs -> FDK weight -> 16-bit hi/lo -> swizzled tiles
+        const int pw = warp - (MMA_WARP + 1);
+        constexpr int ROWS_PW = TILE_M / PROD_WARPS;                    // 16 rows per warp
+        RowInfo* my_rows = rows + pw * ROWS_PW;                         // read by this warp only
+        bool ok = true;
+        int it = 0;
+        for (long long t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++it) {
+            __syncwarp();                                               // previous tile's rows read
+            if (lane < ROWS_PW) {
+                const long long m = t * TILE_M + pw * ROWS_PW + lane;
+                RowInfo ri{};
+                ri.pix = -1;
+                if (m < A.m_total) {
+                    const int v = (int)(m / A.rows);
+                    const int r = (int)(m - (long long)v * A.rows);
+                    const mr_filter_view fv = A.views[v];
+                    const int rr = (RAW && A.flip) ? (A.rows - 1 - r) : r;
+                    const long long off = (long long)v * A.s_view + (long long)rr * (RAW ? A.bin : 1) * A.s_row;
+                    ri.src = RAW ? static_cast<const void*>(static_cast<const uint16_t*>(A.src) + off)
+                                 : static_cast<const void*>(static_cast<const float*>(A.src) + off);
+                    ri.pix = r * A.cols;
+                    ri.sdd = fv.sdd;
+                    ri.a0 = fv.a0;
+                    ri.da = fv.da;
+                    ri.b = fmaf((float)r, fv.db, fv.b0);
+                }
+                my_rows[lane] = ri;
+            }
+            __syncwarp();
+            for (int I = 0; I < KB; ++I) {
+                const uint32_t u = (uint32_t)(it * KB + I);
+                const int s = (int)(u & 1u);
+                if (u >= 2 && !bar_wait(&empty[s], ((u >> 1) & 1u) ^ 1u, abort_flag, A.status)) {
+                    ok = false;
+                    break;
+                }
+                unsigned char* a_hi = a_st + s * STAGE_BYTES;
+                unsigned char* a_lo = a_hi + A_TILE_BYTES;
+                const int c = 64 * I + 2 * lane;
+#pragma unroll 4
+                for (int i = 0; i < ROWS_PW; ++i) {
+                    const int row = pw * ROWS_PW + i;
+                    const RowInfo ri = my_rows[i];
+                    float2 x = make_float2(0.f, 0.f);
+                    if (ri.pix >= 0 && c < A.cols) {
+                        x = load_pair<RAW>(A, ri, c);
+                        x.x *= A.x_scale;
+                        x.y *= A.x_scale;
+                    }
+                    uint32_t hi, lo;
+                    split2<F16>(x, hi, lo);
+                    const uint32_t o = swz(row, 2 * lane);
+                    *reinterpret_cast<uint32_t*>(a_hi + o) = hi;
+                    *reinterpret_cast<uint32_t*>(a_lo + o) = lo;
+                }
+                fence_async_smem();
+                __syncwarp();
+                if (lane == 0) bar_arrive(&full[s]);
+            }
+        }
+    } else if (warp == MMA_WARP) {
+        // ---------------- one thread issues the tensor-core MMAs
+        int it = 0;
+        bool ok = true;
+        for (long long t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++it) {
+            if (it > 0 && !bar_wait(tempty, (uint32_t)(it - 1) & 1u, abort_flag, A.status)) {
+                ok = false;
+                break;
+            }
+            fence_after();
+            for (int I = 0; I < KB && ok; ++I) {
+                const uint32_t u = (uint32_t)(it * KB + I);
+                const int s = (int)(u & 1u);
+                if (!bar_wait(&full[s], (u >> 1) & 1u, abort_flag, A.status)) {
+                    ok = false;
+                    break;
+                }
+                fence_after();
+                if (lane == 0) {
+                    const uint32_t a_hi = smem_addr(a_st + s * STAGE_BYTES);
+                    const uint32_t a_lo = a_hi + A_TILE_BYTES;
+                    const uint32_t bh = smem_addr(b_hi), bl = smem_addr(b_lo);
+                    const int j0 = I > 0 ? I - 1 : 0, j1 = I + 1 < KB ? I + 1 : KB - 1;
+                    const int n_near = 64 * (j1 - j0 + 1);
+                    for (int ks = 0; ks < 4; ++ks) {
+                        const uint32_t kofs = 32u * ks;          // K = 16 step inside the 128-byte row
+                        const uint64_t ah = sdesc(a_hi + kofs), al = sdesc(a_lo + kofs);
+                        // x_hi g_hi over every output column: B rows n + (KB - 1 - I) * 64
+                        for (int n0 = 0; n0 < NCOL; n0 += 256) {
+                            const int n = NCOL - n0 < 256 ? NCOL - n0 : 256;
+                            const uint32_t brow = (uint32_t)(n0 + (KB - 1 - I) * 64);
+                            mma(tmem + n0, ah, sdesc(bh + brow * 128u + kofs), idesc<F16>(n), (I | ks) != 0);
+                        }
+                        // near diagonals: x_hi g_lo and x_lo g_hi for output blocks j0..j1
+                        const uint32_t lrow = (uint32_t)(64 * (j0 - I + 1));
+                        const uint32_t hrow = (uint32_t)(64 * j0 + (KB - 1 - I) * 64);
+                        mma(tmem + 64 * j0, ah, sdesc(bl + lrow * 128u + kofs), idesc<F16>(n_near), 1u);
+                        mma(tmem + 64 * j0, al, sdesc(bh + hrow * 128u + kofs), idesc<F16>(n_near), 1u);
+                    }
+                    mma_commit(&empty[s]);                  // stage s is free once these finish
+                    if (I == KB - 1) mma_commit(tfull);     // accumulator complete
+                }
+                __syncwarp();
+            }
+        }
+        // every MMA this thread issued has completed before tensor memory is released
+        if (lane == 0) mma_commit(drain);
+        __syncwarp();
+        const unsigned long long t0 = global_ns();
+        while (!bar_try(drain, 0u)) {
+            if (global_ns() - t0 > WAIT_NS) {
+                if (A.status) atomicExch(A.status, MR_ERR_TIMEOUT);
+                break;
+            }
+        }
+    } else {
+        // ---------------- epilogue: TMEM -> scale -> ring
+        const int q = warp;                             // TMEM lanes 32q .. 32q + 31
+        int it = 0;
+        for (long long t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+            if (!bar_wait(tfull, (uint32_t)it & 1u, abort_flag, A.status)) break;
+            fence_after();
+            const long long m = t * TILE_M + 32 * q + lane;
+            bool live = m < A.m_total;
+            float scale = 0.f;
+            unsigned char* out = nullptr;
+            if (live) {
+                const int v = (int)(m / A.rows);
+                const int r = (int)(m - (long long)v * A.rows);
+                const mr_filter_view fv = A.views[v];
+                scale = fv.gain * fv.out_scale * A.out_mul;
+                const int esz = A.dtype == MR_F32 ? 4 : 2;
+                live = fv.slot >= 0 && fv.slot < A.n_slots;         // never write outside the ring
+                out = static_cast<unsigned char*>(A.ring) +
+                      ((long long)fv.slot * A.slot_stride + (long long)r * A.pitch) * esz;
+            }
+            const int nch = (A.pitch + 15) / 16;
+            for (int ch = 0; ch < nch; ++ch) {
+                float v[16];
+                if (16 * ch < NCOL) {                               // warp-uniform: inside the accumulator
+                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(16 * ch), v);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) v[e] = 0.f;
+                }
+                if (!live) continue;
+#pragma unroll
+                for (int e = 0; e < 16; ++e) v[e] = (16 * ch + e < A.cols) ? v[e] * scale : 0.f;
+                if (A.dtype == MR_F32) {
+#pragma unroll
+                    for (int h = 0; h < 4; ++h)
+                        if (16 * ch + 4 * h + 4 <= A.pitch)
+                            *reinterpret_cast<float4*>(out + (16 * ch + 4 * h) * 4) =
+                                make_float4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
+                } else {
+                    uint32_t w[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        if (A.dtype == MR_BF16) {
+                            const __nv_bfloat162 p = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
+                            w[e] = *reinterpret_cast<const uint32_t*>(&p);
+                        } else {
+                            const __half2 p = __floats2half2_rn(v[2 * e], v[2 * e + 1]);
+                            w[e] = *reinterpret_cast<const uint32_t*>(&p);
+                        }
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        if (16 * ch + 8 * h + 8 <= A.pitch)
+                            *reinterpret_cast<uint4*>(out + (16 * ch + 8 * h) * 2) =
+                                make_uint4(w[4 * h], w[4 * h + 1], w[4 * h + 2], w[4 * h + 3]);
+                }
+            }
+            fence_before();
+            __syncwarp();
+            if (lane == 0) bar_arrive(tempty);
+        }
+    }
+
+    __syncthreads();
+    if (warp == MMA_WARP) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+    }
+}
+
+inline size_t smem_bytes(int kb) {
+    return 1024 + (size_t)(2 * kb - 1 + 3) * BLOCK_BYTES + (size_t)STAGES * STAGE_BYTES + TILE_M * sizeof(RowInfo) +
+           (2 * STAGES + 3) * sizeof(uint64_t) + 16;
+}
+
+template <bool RAW>
+static int launch(Args& A, bool f16, cudaStream_t st) {
+    const size_t smem = smem_bytes(A.kb);
+    auto kern = f16 ? toeplitz_tc_kernel<RAW, true> : toeplitz_tc_kernel<RAW, false>;
+    MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 148;
+    MR_CUDA_TRY(cudaGetDevice(&dev));
+    MR_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long long n_tiles = (A.m_total + TILE_M - 1) / TILE_M;
+    if (n_tiles <= 0) return MR_OK;
+    const unsigned grid = (unsigned)(n_tiles < sms ? n_tiles : sms);
+    kern<<<grid, THREADS, smem, st>>>(A);
+    MR_CUDA_TRY(cudaGetLastError());
+    return MR_OK;
+}
+
+static int check_ring(const mr_ring* ring, int32_t k, const mr_filter_view* views, const void* bimg, int32_t n_fft) {
+    if (!ring || !ring->data || !views || !bimg || k < 0) return MR_ERR_INVALID;
+    if (ring->rows <= 0 || ring->cols <= 0 || ring->col_pitch < ring->cols) return MR_ERR_INVALID;
+    if (ring->slot_stride < (int64_t)ring->rows * ring->col_pitch) return MR_ERR_INVALID;
+    if (ring->dtype != MR_F32 && ring->dtype != MR_BF16 && ring->dtype != MR_F16) return MR_ERR_INVALID;
+    if (ring->col_pitch % 8 || ring->slot_stride % 8 || (reinterpret_cast<uintptr_t>(ring->data) & 15))
+        return MR_ERR_INVALID;
+    if (n_fft < 2 * ring->cols || (n_fft & (n_fft - 1))) return MR_ERR_INVALID;
+    if ((reinterpret_cast<uintptr_t>(bimg) & 15)) return MR_ERR_INVALID;
+    if (ring->cols > 64 * KB_MAX) return MR_ERR_UNSUPPORTED;
+    return MR_OK;
+}
+
+static void fill(Args& A, const mr_ring* ring, int32_t k, const mr_filter_view* views, const void* bimg,
+                 int32_t n_fft, float t_scale, float x_scale, int32_t* status) {
+    A.views = views;
+    A.bimg = static_cast<const unsigned char*>(bimg);
+    A.x_scale = x_scale;
+    A.out_mul = (float)((double)n_fft / ((double)x_scale * (double)t_scale));
+    A.ring = ring->data;
+    A.dtype = ring->dtype;
+    A.rows = ring->rows;
+    A.cols = ring->cols;
+    A.pitch = ring->col_pitch;
+    A.n_slots = ring->n_slots;
+    A.slot_stride = ring->slot_stride;
+    A.m_total = (long long)k * ring->rows;
+    A.kb = (ring->cols + 63) / 64;
+    A.status = status;
+}
+
+static inline uint16_t bf16_bits(double x) {
+    // round-to-nearest-even of the FP32 value to BF16 (finite inputs)
+    float f = (float)x;
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+static inline double bf16_value(uint16_t b) {
+    uint32_t u = (uint32_t)b << 16;
+    float f;
+    memcpy(&f, &u, 4);
+    return (double)f;
+}
+static inline uint16_t f16_bits(double x) { return __half_as_ushort(__float2half_rn((float)x)); }
+static inline double f16_value(uint16_t b) { return (double)__half2float(__ushort_as_half(b)); }
+
+static bool pow2_scale(float s) {
+    if (!(s > 0.f) || !isfinite(s)) return false;
+    int e = 0;
+    return frexpf(s, &e) == 0.5f;
+}
+
+}  // namespace tc
+}  // namespace mr
+
+extern "C" int64_t mr_toeplitz_image_bytes(int32_t cols) {
+    if (cols <= 0 || cols > 64 * mr::tc::KB_MAX) return -1;
+    const int kb = (cols + 63) / 64;
+    return (int64_t)(2 * kb - 1 + 3) * mr::tc::BLOCK_BYTES;
+}
+
+extern "C" int mr_toeplitz_image(const double* g, int32_t n_fft, int32_t cols, int32_t format, void* image,
+                                 float* t_scale) {
+    using namespace mr::tc;
+    if (!g || !image || !t_scale || cols <= 0 || n_fft < 2 * cols || (n_fft & (n_fft - 1))) return MR_ERR_INVALID;
+    if (format != MR_F16 && format != MR_BF16) return MR_ERR_INVALID;
+    if (cols > 64 * KB_MAX) return MR_ERR_UNSUPPORTED;
+    const int kb = (cols + 63) / 64;
+    // power-of-two scale putting max |g| in [2^13, 2^14): FP16 normal range for the hi
+    // parts and the near-diagonal lo parts (BF16 gets the same scale; its range makes it moot)
+    double gmax = 0.0;
+    for (int i = 0; i < n_fft; ++i) gmax = fmax(gmax, fabs(g[i]));
+    int e = 0;
+    if (gmax > 0.0) {
+        frexp(gmax, &e);                        // gmax = m 2^e, m in [0.5, 1)
+        e = 14 - e;
+        if (e > 100) e = 100;
+        if (e < -100) e = -100;
+    }
+    const double s = ldexp(1.0, e);
+    *t_scale = (float)s;
+    unsigned char* img = static_cast<unsigned char*>(image);
+    memset(img, 0, (size_t)mr_toeplitz_image_bytes(cols));
+    unsigned char* lo_base = img + (size_t)(2 * kb - 1) * BLOCK_BYTES;
+    const bool f16 = format == MR_F16;
+    for (int d = -(kb - 1); d <= kb - 1; ++d) {
+        for (int r = 0; r < 64; ++r) {
+            for (int k = 0; k < 64; ++k) {
+                const int idx = ((64 * d + r - k) % n_fft + n_fft) % n_fft;
+                const double val = g[idx] * s;
+                const uint16_t hi = f16 ? f16_bits(val) : bf16_bits(val);
+                const int row = (d + kb - 1) * 64 + r;
+                const size_t off = (size_t)(row >> 3) * 1024 + (row & 7) * 128 + ((((k >> 3) ^ (row & 7)) & 7) << 4) +
+                                   (k & 7) * 2;
+                memcpy(img + off, &hi, 2);
+                if (d >= -1 && d <= 1) {
+                    const double rest = val - (f16 ? f16_value(hi) : bf16_value(hi));
+                    const uint16_t lo = f16 ? f16_bits(rest) : bf16_bits(rest);
+                    const int lrow = (d + 1) * 64 + r;
+                    const size_t loff = (size_t)(lrow >> 3) * 1024 + (lrow & 7) * 128 +
+                                        ((((k >> 3) ^ (lrow & 7)) & 7) << 4) + (k & 7) * 2;
+                    memcpy(lo_base + loff, &lo, 2);
+                }
+            }
+        }
+    }
+    return MR_OK;
+}
+
+extern "C" int mr_filter_f32_tc(const float* block, int64_t s_view, int64_t s_row, int32_t k,
+                                const mr_filter_view* views, const void* image, int32_t format, float t_scale,
+                                float x_scale, int32_t n_fft, const mr_ring* ring, int32_t* status, void* stream) {
+    int rc = mr::tc::check_ring(ring, k, views, image, n_fft);
+    if (rc != MR_OK) return rc;
+    if (!block || s_row < 1 || s_view < 1) return MR_ERR_INVALID;
+    if ((format != MR_F16 && format != MR_BF16) || !mr::tc::pow2_scale(t_scale) || !mr::tc::pow2_scale(x_scale))
+        return MR_ERR_INVALID;
+    if (k == 0) return MR_OK;
+    mr::tc::Args A{};
+    mr::tc::fill(A, ring, k, views, image, n_fft, t_scale, x_scale, status);
+    A.src = block;
+    A.s_view = s_view;
+    A.s_row = s_row;
+    A.bin = 1;
+    A.vec_src = (s_view % 2 == 0) && (s_row % 2 == 0) && ((reinterpret_cast<uintptr_t>(block) & 7) == 0);
+    return mr::tc::launch<false>(A, format == MR_F16, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int mr_ingest_u16_tc(const uint16_t* raw, int64_t s_view, int64_t s_row, int32_t bin, int32_t flip_rows,
+                                const float* dark, const float* gain, int32_t k, const mr_filter_view* views,
+                                const void* image, int32_t format, float t_scale, int32_t n_fft,
+                                const mr_ring* ring, int32_t* status, void* stream) {
+    int rc = mr::tc::check_ring(ring, k, views, image, n_fft);
+    if (rc != MR_OK) return rc;
+    if (!raw || !dark || !gain || bin < 1 || bin > 16) return MR_ERR_INVALID;
+    if (s_row < (int64_t)ring->cols * bin || s_view < 1) return MR_ERR_INVALID;
+    if ((format != MR_F16 && format != MR_BF16) || !mr::tc::pow2_scale(t_scale)) return MR_ERR_INVALID;
+    if (k == 0) return MR_OK;
+    mr::tc::Args A{};
+    // -log(max(t, 1e-3)) lies in [-log(65535), log(1000)] and the FDK weight is <= 1, so
+    // |x| < 11.1: 1024 |x| stays inside FP16's range with its lo part mostly normal
+    mr::tc::fill(A, ring, k, views, image, n_fft, t_scale, 1024.f, status);
+    A.src = raw;
+    A.s_view = s_view;
+    A.s_row = s_row;
+    A.bin = bin;
+    A.flip = flip_rows != 0;
+    A.dark = dark;
+    A.gain = gain;
+    A.vec_src = bin == 1 && (s_view % 2 == 0) && (s_row % 2 == 0) && ((reinterpret_cast<uintptr_t>(raw) & 3) == 0);
+    A.vec_fld = (ring->cols % 2 == 0) && ((reinterpret_cast<uintptr_t>(dark) & 7) == 0) &&
+                ((reinterpret_cast<uintptr_t>(gain) & 7) == 0);
+    return mr::tc::launch<true>(A, format == MR_F16, static_cast<cudaStream_t>(stream));
+}

@@ -11,6 +11,7 @@ FP64 is used on the host only, to build the per-view projective maps and the fil
 spectrum (as the reference does); the device computes in FP32 and stores the filtered
 views in FP32 (default), BF16 or FP16.
 """
+import ctypes
 import threading
 import time
 
@@ -68,6 +69,28 @@ class _FilterTables:
         self.log2n = int(round(np.log2(n_fft)))
         self.H = torch.from_numpy(full.astype(np.float32)).to(device)
         self.tw = torch.from_numpy(np.stack([tw.real, tw.imag], 1).astype(np.float32)).to(device)
+        self._full64 = full
+        self._cols = cols
+        self._device = device
+        self._tc_image = {}
+
+    def tc_image(self, fmt=None):
+        """(device operand, t_scale) of the tensor-core Toeplitz filter (mr_toeplitz_image):
+        the split FP16 (default) or BF16 blocks of g = ifft(H) (tau = 1, FP64 on the host),
+        built on first use."""
+        fmt = N.MR_F16 if fmt is None else fmt
+        if fmt not in self._tc_image:
+            lib = N.load()
+            nbytes = lib.mr_toeplitz_image_bytes(self._cols)
+            if nbytes < 0:
+                raise ValueError(f"the tensor-core filter supports rows of at most 512 columns, not {self._cols}")
+            g = np.ascontiguousarray(np.fft.ifft(self._full64).real, dtype=np.float64)
+            img = np.zeros(nbytes, dtype=np.uint8)
+            ts = ctypes.c_float()
+            N.check(lib.mr_toeplitz_image(g.ctypes.data, self.n_fft, self._cols, fmt, img.ctypes.data,
+                                          ctypes.byref(ts)), "mr_toeplitz_image")
+            self._tc_image[fmt] = (torch.from_numpy(img).to(self._device), float(ts.value))
+        return self._tc_image[fmt]
 
 
 # --------------------------------------------------------------------------
@@ -208,9 +231,23 @@ def _struct_tensor(records, device):
     return torch.from_numpy(raw.copy()).to(device, non_blocking=False)
 
 
-def filter_block_device(block, s_view, s_row, k, fviews_dev, tables, ring, stream):
-    """Filter k views of a device f32 block into ring slots (mr_filter_f32)."""
+def filter_block_device(block, s_view, s_row, k, fviews_dev, tables, ring, stream, method="fft", status=None):
+    """Filter k views of a device f32 block into ring slots: mr_filter_f32 (FFT) or
+    mr_filter_f32_tc (tensor-core Toeplitz GEMM, split FP16 "tc" or split BF16 "tc-bf16")."""
     lib = N.load()
+    if method in ("tc", "tc-bf16"):
+        fmt = N.MR_BF16 if method == "tc-bf16" else N.MR_F16
+        img, t_scale = tables.tc_image(fmt)
+        # power of two with max |x| * x_scale in [2^13, 2^14) (FP16 range for the hi part)
+        m = float(block.abs().amax()) if block.numel() else 0.0
+        x_scale = 2.0 ** int(np.clip(14 - np.frexp(m)[1], -100, 100)) if m > 0 and np.isfinite(m) else 1.0
+        st = lib.mr_filter_f32_tc(ctypes_void(block.data_ptr()), s_view, s_row, k,
+                                  ctypes_void(fviews_dev.data_ptr()), ctypes_void(img.data_ptr()), fmt, t_scale,
+                                  x_scale, tables.n_fft, ring,
+                                  ctypes_void(status.data_ptr()) if status is not None else None,
+                                  ctypes_void(stream.cuda_stream))
+        N.check(st, "mr_filter_f32_tc")
+        return
     st = lib.mr_filter_f32(ctypes_void(block.data_ptr()), s_view, s_row, k,
                            ctypes_void(fviews_dev.data_ptr()), ctypes_void(tables.H.data_ptr()),
                            ctypes_void(tables.tw.data_ptr()), tables.log2n, ring,
@@ -441,16 +478,25 @@ class SliceReconstructor:
     tilt     : detector tilt correction in degrees (rotates each projection).
     store    : filtered-view storage, "fp32" (default), "bf16" or "fp16".
     device   : CUDA device (default: the current one).
+    filter   : "fft" (default; shared-memory FFT, FP32), "tc" (Toeplitz GEMM on the tensor
+               cores, split FP16 operands, FP32 accumulation; rows <= 512 columns) or
+               "tc-bf16" (the same with split BF16 operands, ~100x less precise on
+               smooth rows because the ramp filter cancels strongly).
     The `backend` argument is accepted for compatibility; the backend is always
     "cuda-sm100a".
     """
 
     def __init__(self, proj=None, geom=None, window="shepp-logan", backend="auto",
-                 gaussian=0.0, tilt=0.0, verbose=True, store="fp32", device=None):
+                 gaussian=0.0, tilt=0.0, verbose=True, store="fp32", device=None, filter="fft"):
         if geom is None:
             raise ValueError("geometry is required")
         if store not in _STORE_DTYPES:
             raise ValueError(f"unknown store {store!r}: use one of {sorted(_STORE_DTYPES)}")
+        if filter not in ("fft", "tc", "tc-bf16"):
+            raise ValueError(f"unknown filter {filter!r}: use 'fft', 'tc' or 'tc-bf16'")
+        if filter != "fft" and geom.cols > 512:
+            raise ValueError("the tensor-core filter supports detector rows of at most 512 columns")
+        self.filter_method = filter
         self.device = _device(device)
         N.load()
         self.requested_backend = backend
@@ -571,7 +617,7 @@ class SliceReconstructor:
                 x, s_view, s_row = preprocess.apply_device(x, self.gaussian, self.tilt)
                 fv = _struct_tensor(self._filter_views(indices, slots), self.device)
                 filter_block_device(x, s_view, s_row, k, fv, self._tables, self._ring_c,
-                                    self.ingest_stream)
+                                    self.ingest_stream, self.filter_method, self._status)
                 ev = torch.cuda.Event()
             return self._admit(indices, slots, ev)
 
@@ -669,17 +715,25 @@ class SliceReconstructor:
         lib = N.load()
         t = self._tables
         tm = self.kernel_timer
+        name = "mr_ingest_u16" if self.filter_method == "fft" else "mr_ingest_u16_tc"
         ev0 = tm.start(self.ingest_stream) if tm is not None else None
         view_bytes = x.shape[1] * x.shape[2] * 2
-        st = lib.mr_ingest_u16(ctypes_void(x.data_ptr() + c0 * view_bytes), x.shape[1] * x.shape[2], x.shape[2],
-                               self._raw_bin, int(self._raw_flip), ctypes_void(self._dark.data_ptr()),
-                               ctypes_void(self._gain.data_ptr()), c1 - c0,
-                               ctypes_void(fv.data_ptr() + c0 * N.FILTER_VIEW_DTYPE.itemsize),
-                               ctypes_void(t.H.data_ptr()), ctypes_void(t.tw.data_ptr()), t.log2n,
-                               self._ring_c, ctypes_void(self.ingest_stream.cuda_stream))
+        common = (ctypes_void(x.data_ptr() + c0 * view_bytes), x.shape[1] * x.shape[2], x.shape[2],
+                  self._raw_bin, int(self._raw_flip), ctypes_void(self._dark.data_ptr()),
+                  ctypes_void(self._gain.data_ptr()), c1 - c0,
+                  ctypes_void(fv.data_ptr() + c0 * N.FILTER_VIEW_DTYPE.itemsize))
+        if self.filter_method == "fft":
+            st = lib.mr_ingest_u16(*common, ctypes_void(t.H.data_ptr()), ctypes_void(t.tw.data_ptr()), t.log2n,
+                                   self._ring_c, ctypes_void(self.ingest_stream.cuda_stream))
+        else:
+            fmt = N.MR_BF16 if self.filter_method == "tc-bf16" else N.MR_F16
+            img, t_scale = t.tc_image(fmt)
+            st = lib.mr_ingest_u16_tc(*common, ctypes_void(img.data_ptr()), fmt, t_scale, t.n_fft, self._ring_c,
+                                      ctypes_void(self._status.data_ptr()),
+                                      ctypes_void(self.ingest_stream.cuda_stream))
         if tm is not None:
-            tm.stop("mr_ingest_u16", ev0, self.ingest_stream)
-        N.check(st, "mr_ingest_u16")
+            tm.stop(name, ev0, self.ingest_stream)
+        N.check(st, name)
 
     def _ingest_host(self, raw, k, fv):
         """Upload host raw counts in chunks on the copy stream and filter each chunk on the
