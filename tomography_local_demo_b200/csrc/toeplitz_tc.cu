@@ -6,7 +6,7 @@
 // linear map y = T x with T[n][j] = g[(n - j) mod N], g = ifft(H) - a C x C Toeplitz
 // matrix - so filtering a stack of rows is one dense GEMM  Y[rows, C] = X[rows, C] T^T.
 //
-// Layout of the contraction (one 128-row tile of detector rows per pass):
+// Layout of the contraction (one tile = one detector row of up to 128 views per pass):
 //   * K and N are cut into 64-wide blocks; block (J, I) of T depends only on d = J - I,
 //     so the whole operand is 2*KB - 1 distinct 64 x 64 blocks (KB = ceil(C / 64) <= 8).
 //     They stay resident in shared memory for the CTA's lifetime (<= 120 KB).
@@ -30,6 +30,8 @@
 
 #include <math.h>
 #include <string.h>
+
+#include <type_traits>
 
 namespace mr {
 namespace tc {
@@ -67,7 +69,7 @@ struct Args {
     void* ring;
     int dtype, rows, cols, pitch, n_slots;
     long long slot_stride;
-    long long m_total;                          // k * rows
+    int k;                                      // views in this launch
     int kb;
     int vec_src, vec_fld;                       // 4-byte raw pairs / 8-byte float pairs usable
     int* status;
@@ -141,18 +143,21 @@ __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::aft
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
     // load and wait in one statement: the outputs are defined only once the load is complete
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
         "tcgen05.wait::ld.sync.aligned;"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr)
         : "memory");
 #pragma unroll
-    for (int e = 0; e < 16; ++e) v[e] = __uint_as_float(r[e]);
+    for (int e = 0; e < 32; ++e) v[e] = __uint_as_float(r[e]);
 }
 
 // Byte offset of element (row, k) (k even: a pair of 16-bit values) in a SWIZZLE_128B
@@ -285,24 +290,29 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tmem_slot;
-    const long long n_tiles = (A.m_total + TILE_M - 1) / TILE_M;
+    // a tile is one detector row r of up to 128 consecutive views: the GEMM rows of a tile
+    // share the row's dark / gain fields and FDK row term, so they are loaded once per tile
+    const long long n_tiles = (long long)A.rows * ((A.k + TILE_M - 1) / TILE_M);
 
     if (warp >= MMA_WARP + 1) {
         // ---------------- producers: inputs -> FDK weight -> 16-bit hi/lo -> swizzled tiles
         const int pw = warp - (MMA_WARP + 1);
-        constexpr int ROWS_PW = TILE_M / PROD_WARPS;                    // 16 rows per warp
-        RowInfo* my_rows = rows + pw * ROWS_PW;                         // read by this warp only
+        constexpr int RPW = TILE_M / PROD_WARPS;                        // 16 rows (views) per warp
+        RowInfo* my_rows = rows + pw * RPW;                             // read by this warp only
+        // vector path: a lane's column pair is one aligned 4-byte (raw) / 8-byte (FP32) load
+        const bool fast = RAW ? (A.bin == 1 && A.vec_src && A.vec_fld) : (A.vec_src && (A.cols % 2 == 0));
+        using Pair = typename std::conditional<RAW, uint32_t, float2>::type;
         bool ok = true;
         int it = 0;
         for (long long t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, ++it) {
+            const int r = (int)(t % A.rows);
+            const int vb = (int)(t / A.rows);
             __syncwarp();                                               // previous tile's rows read
-            if (lane < ROWS_PW) {
-                const long long m = t * TILE_M + pw * ROWS_PW + lane;
+            if (lane < RPW) {
+                const int v = vb * TILE_M + pw * RPW + lane;
                 RowInfo ri{};
                 ri.pix = -1;
-                if (m < A.m_total) {
-                    const int v = (int)(m / A.rows);
-                    const int r = (int)(m - (long long)v * A.rows);
+                if (v < A.k) {
                     const mr_filter_view fv = A.views[v];
                     const int rr = (RAW && A.flip) ? (A.rows - 1 - r) : r;
                     const long long off = (long long)v * A.s_view + (long long)rr * (RAW ? A.bin : 1) * A.s_row;
@@ -317,35 +327,114 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                 my_rows[lane] = ri;
             }
             __syncwarp();
-            for (int I = 0; I < KB; ++I) {
-                const uint32_t u = (uint32_t)(it * KB + I);
-                const int s = (int)(u & 1u);
-                if (u >= 2 && !bar_wait(&empty[s], ((u >> 1) & 1u) ^ 1u, abort_flag, A.status)) {
-                    ok = false;
-                    break;
-                }
-                unsigned char* a_hi = a_st + s * STAGE_BYTES;
-                unsigned char* a_lo = a_hi + A_TILE_BYTES;
-                const int c = 64 * I + 2 * lane;
-#pragma unroll 4
-                for (int i = 0; i < ROWS_PW; ++i) {
-                    const int row = pw * ROWS_PW + i;
-                    const RowInfo ri = my_rows[i];
-                    float2 x = make_float2(0.f, 0.f);
-                    if (ri.pix >= 0 && c < A.cols) {
-                        x = load_pair<RAW>(A, ri, c);
-                        x.x *= A.x_scale;
-                        x.y *= A.x_scale;
+            if (fast) {
+                // software pipeline: the loads of K-block I + 1 are in flight while block I
+                // is converted, so each warp keeps 16 rows x 2 blocks of requests outstanding
+                Pair cur[RPW], nxt[RPW];
+#pragma unroll
+                for (int i = 0; i < RPW; ++i) nxt[i] = Pair{};
+                float2 dk_c = make_float2(0.f, 0.f), gn_c = dk_c, dk_n = dk_c, gn_n = dk_c;
+                auto issue = [&](int I, Pair* buf, float2& dk, float2& gn) {
+                    const int c = 64 * I + 2 * lane;
+                    const bool cin = c < A.cols;
+#pragma unroll
+                    for (int i = 0; i < RPW; ++i) {
+                        const void* src = my_rows[i].src;
+                        const bool live = cin && my_rows[i].pix >= 0;
+                        if (RAW) {
+                            uint32_t w = 0u;
+                            if (live) w = __ldg(reinterpret_cast<const unsigned int*>(static_cast<const uint16_t*>(src) + c));
+                            reinterpret_cast<uint32_t*>(buf)[i] = w;
+                        } else {
+                            float2 w = make_float2(0.f, 0.f);
+                            if (live) w = __ldg(reinterpret_cast<const float2*>(static_cast<const float*>(src) + c));
+                            reinterpret_cast<float2*>(buf)[i] = w;
+                        }
                     }
-                    uint32_t hi, lo;
-                    split2<F16>(x, hi, lo);
-                    const uint32_t o = swz(row, 2 * lane);
-                    *reinterpret_cast<uint32_t*>(a_hi + o) = hi;
-                    *reinterpret_cast<uint32_t*>(a_lo + o) = lo;
+                    if (RAW && cin) {
+                        dk = __ldg(reinterpret_cast<const float2*>(A.dark + r * A.cols + c));
+                        gn = __ldg(reinterpret_cast<const float2*>(A.gain + r * A.cols + c));
+                    }
+                };
+                issue(0, cur, dk_c, gn_c);
+                for (int I = 0; I < KB; ++I) {
+                    if (I + 1 < KB) issue(I + 1, nxt, dk_n, gn_n);
+                    const uint32_t u = (uint32_t)(it * KB + I);
+                    const int s = (int)(u & 1u);
+                    if (u >= 2 && !bar_wait(&empty[s], ((u >> 1) & 1u) ^ 1u, abort_flag, A.status)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char* a_hi = a_st + s * STAGE_BYTES;
+                    unsigned char* a_lo = a_hi + A_TILE_BYTES;
+                    const int c = 64 * I + 2 * lane;
+                    const bool cin = c < A.cols;
+                    const float fc1 = (float)c, fc2 = (float)(c + 1);
+#pragma unroll
+                    for (int i = 0; i < RPW; ++i) {
+                        const RowInfo ri = my_rows[i];
+                        float2 x = make_float2(0.f, 0.f);
+                        if (cin && ri.pix >= 0) {
+                            if (RAW) {
+                                const uint32_t w = reinterpret_cast<const uint32_t*>(cur)[i];
+                                x.x = -__logf(fmaxf(((float)(w & 0xFFFFu) - dk_c.x) * gn_c.x, 1e-3f));
+                                x.y = -__logf(fmaxf(((float)(w >> 16) - dk_c.y) * gn_c.y, 1e-3f));
+                            } else {
+                                x = reinterpret_cast<const float2*>(cur)[i];
+                            }
+                            if (ri.sdd != 0.f) {
+                                const float a1 = fmaf(fc1, ri.da, ri.a0), a2 = fmaf(fc2, ri.da, ri.a0);
+                                x.x *= ri.sdd * rsqrtf(fmaf(ri.b, ri.b, fmaf(ri.sdd, ri.sdd, a1 * a1)));
+                                x.y *= ri.sdd * rsqrtf(fmaf(ri.b, ri.b, fmaf(ri.sdd, ri.sdd, a2 * a2)));
+                            }
+                            x.x *= A.x_scale;
+                            x.y *= A.x_scale;
+                        }
+                        uint32_t hi, lo;
+                        split2<F16>(x, hi, lo);
+                        const uint32_t o = swz(pw * RPW + i, 2 * lane);
+                        *reinterpret_cast<uint32_t*>(a_hi + o) = hi;
+                        *reinterpret_cast<uint32_t*>(a_lo + o) = lo;
+                    }
+                    fence_async_smem();
+                    __syncwarp();
+                    if (lane == 0) bar_arrive(&full[s]);
+#pragma unroll
+                    for (int i = 0; i < RPW; ++i) cur[i] = nxt[i];
+                    dk_c = dk_n;
+                    gn_c = gn_n;
                 }
-                fence_async_smem();
-                __syncwarp();
-                if (lane == 0) bar_arrive(&full[s]);
+            } else {
+                // general path (binning, unaligned rows, odd widths): element loads
+                for (int I = 0; I < KB; ++I) {
+                    const uint32_t u = (uint32_t)(it * KB + I);
+                    const int s = (int)(u & 1u);
+                    if (u >= 2 && !bar_wait(&empty[s], ((u >> 1) & 1u) ^ 1u, abort_flag, A.status)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char* a_hi = a_st + s * STAGE_BYTES;
+                    unsigned char* a_lo = a_hi + A_TILE_BYTES;
+                    const int c = 64 * I + 2 * lane;
+#pragma unroll 4
+                    for (int i = 0; i < RPW; ++i) {
+                        const RowInfo ri = my_rows[i];
+                        float2 x = make_float2(0.f, 0.f);
+                        if (ri.pix >= 0 && c < A.cols) {
+                            x = load_pair<RAW>(A, ri, c);
+                            x.x *= A.x_scale;
+                            x.y *= A.x_scale;
+                        }
+                        uint32_t hi, lo;
+                        split2<F16>(x, hi, lo);
+                        const uint32_t o = swz(pw * RPW + i, 2 * lane);
+                        *reinterpret_cast<uint32_t*>(a_hi + o) = hi;
+                        *reinterpret_cast<uint32_t*>(a_lo + o) = lo;
+                    }
+                    fence_async_smem();
+                    __syncwarp();
+                    if (lane == 0) bar_arrive(&full[s]);
+                }
             }
         }
     } else if (warp == MMA_WARP) {
@@ -410,13 +499,12 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
         for (long long t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
             if (!bar_wait(tfull, (uint32_t)it & 1u, abort_flag, A.status)) break;
             fence_after();
-            const long long m = t * TILE_M + 32 * q + lane;
-            bool live = m < A.m_total;
+            const int r = (int)(t % A.rows);
+            const int v = (int)(t / A.rows) * TILE_M + 32 * q + lane;
+            bool live = v < A.k;
             float scale = 0.f;
             unsigned char* out = nullptr;
             if (live) {
-                const int v = (int)(m / A.rows);
-                const int r = (int)(m - (long long)v * A.rows);
                 const mr_filter_view fv = A.views[v];
                 scale = fv.gain * fv.out_scale * A.out_mul;
                 const int esz = A.dtype == MR_F32 ? 4 : 2;
@@ -424,40 +512,40 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                 out = static_cast<unsigned char*>(A.ring) +
                       ((long long)fv.slot * A.slot_stride + (long long)r * A.pitch) * esz;
             }
-            const int nch = (A.pitch + 15) / 16;
+            const int nch = (A.pitch + 31) / 32;
             for (int ch = 0; ch < nch; ++ch) {
-                float v[16];
-                if (16 * ch < NCOL) {                               // warp-uniform: inside the accumulator
-                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(16 * ch), v);
+                float vv[32];
+                if (32 * ch < NCOL) {                               // warp-uniform: inside the accumulator
+                    tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * ch), vv);
                 } else {
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) v[e] = 0.f;
+                    for (int e = 0; e < 32; ++e) vv[e] = 0.f;
                 }
                 if (!live) continue;
 #pragma unroll
-                for (int e = 0; e < 16; ++e) v[e] = (16 * ch + e < A.cols) ? v[e] * scale : 0.f;
+                for (int e = 0; e < 32; ++e) vv[e] = (32 * ch + e < A.cols) ? vv[e] * scale : 0.f;
                 if (A.dtype == MR_F32) {
 #pragma unroll
-                    for (int h = 0; h < 4; ++h)
-                        if (16 * ch + 4 * h + 4 <= A.pitch)
-                            *reinterpret_cast<float4*>(out + (16 * ch + 4 * h) * 4) =
-                                make_float4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
+                    for (int h = 0; h < 8; ++h)
+                        if (32 * ch + 4 * h + 4 <= A.pitch)
+                            *reinterpret_cast<float4*>(out + (32 * ch + 4 * h) * 4) =
+                                make_float4(vv[4 * h], vv[4 * h + 1], vv[4 * h + 2], vv[4 * h + 3]);
                 } else {
-                    uint32_t w[8];
+                    uint32_t w[16];
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) {
+                    for (int e = 0; e < 16; ++e) {
                         if (A.dtype == MR_BF16) {
-                            const __nv_bfloat162 p = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
-                            w[e] = *reinterpret_cast<const uint32_t*>(&p);
+                            const __nv_bfloat162 pk = __floats2bfloat162_rn(vv[2 * e], vv[2 * e + 1]);
+                            w[e] = *reinterpret_cast<const uint32_t*>(&pk);
                         } else {
-                            const __half2 p = __floats2half2_rn(v[2 * e], v[2 * e + 1]);
-                            w[e] = *reinterpret_cast<const uint32_t*>(&p);
+                            const __half2 pk = __floats2half2_rn(vv[2 * e], vv[2 * e + 1]);
+                            w[e] = *reinterpret_cast<const uint32_t*>(&pk);
                         }
                     }
 #pragma unroll
-                    for (int h = 0; h < 2; ++h)
-                        if (16 * ch + 8 * h + 8 <= A.pitch)
-                            *reinterpret_cast<uint4*>(out + (16 * ch + 8 * h) * 2) =
+                    for (int h = 0; h < 4; ++h)
+                        if (32 * ch + 8 * h + 8 <= A.pitch)
+                            *reinterpret_cast<uint4*>(out + (32 * ch + 8 * h) * 2) =
                                 make_uint4(w[4 * h], w[4 * h + 1], w[4 * h + 2], w[4 * h + 3]);
                 }
             }
@@ -487,7 +575,7 @@ static int launch(Args& A, bool f16, cudaStream_t st) {
     int dev = 0, sms = 148;
     MR_CUDA_TRY(cudaGetDevice(&dev));
     MR_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const long long n_tiles = (A.m_total + TILE_M - 1) / TILE_M;
+    const long long n_tiles = (long long)A.rows * ((A.k + TILE_M - 1) / TILE_M);
     if (n_tiles <= 0) return MR_OK;
     const unsigned grid = (unsigned)(n_tiles < sms ? n_tiles : sms);
     kern<<<grid, THREADS, smem, st>>>(A);
@@ -521,7 +609,7 @@ static void fill(Args& A, const mr_ring* ring, int32_t k, const mr_filter_view* 
     A.pitch = ring->col_pitch;
     A.n_slots = ring->n_slots;
     A.slot_stride = ring->slot_stride;
-    A.m_total = (long long)k * ring->rows;
+    A.k = k;
     A.kb = (ring->cols + 63) / 64;
     A.status = status;
 }
