@@ -131,6 +131,9 @@ typedef struct mr_filter_view {
 /* ---- library information ------------------------------------------------------- */
 int         mr_abi_version(void);
 const char* mr_status_string(int status);
+/* Text of the CUDA error behind the last MR_ERR_CUDA returned on the calling host
+ * thread ("" if none). */
+const char* mr_last_cuda_error(void);
 /* sizeof() of the ABI structs, for layout checks by bindings:
  * which = 0 mr_ring, 1 mr_view, 2 mr_grid, 3 mr_tile, 4 mr_filter_view; -1 otherwise. */
 int         mr_struct_size(int which);

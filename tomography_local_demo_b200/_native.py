@@ -52,6 +52,7 @@ _I32, _I64 = ctypes.c_int32, ctypes.c_int64
 SIGNATURES = {
     "mr_abi_version": (ctypes.c_int, []),
     "mr_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "mr_last_cuda_error": (ctypes.c_char_p, []),
     "mr_struct_size": (ctypes.c_int, [ctypes.c_int]),
     "mr_bp_tile_shape": (None, [ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
     "mr_plan_tiles": (ctypes.c_int, [_P, _I32, _P, _I64, ctypes.POINTER(_I64)]),
@@ -117,6 +118,8 @@ def check(status, what):
     if status == MR_OK:
         return
     msg = f"{what}: {load().mr_status_string(status).decode()} (status {status})"
+    if status == MR_ERR_CUDA:
+        msg += f": {load().mr_last_cuda_error().decode()}"
     if status == MR_ERR_INVALID:
         raise ValueError(msg)
     if status == MR_ERR_TIMEOUT:

@@ -1,7 +1,16 @@
 // Library information entry points of the C ABI.
 #include "mr_common.cuh"
 
+namespace mr {
+static thread_local cudaError_t g_last_cuda_error = cudaSuccess;
+void set_last_cuda_error(cudaError_t e) { g_last_cuda_error = e; }
+}  // namespace mr
+
 extern "C" int mr_abi_version(void) { return MR_ABI_VERSION; }
+
+extern "C" const char* mr_last_cuda_error(void) {
+    return mr::g_last_cuda_error == cudaSuccess ? "" : cudaGetErrorString(mr::g_last_cuda_error);
+}
 
 extern "C" const char* mr_status_string(int status) {
     switch (status) {

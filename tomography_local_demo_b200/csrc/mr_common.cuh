@@ -8,10 +8,18 @@
 
 #include "minirecast_b200.h"
 
+namespace mr {
+// The CUDA error behind the last MR_ERR_CUDA returned on this host thread.
+void set_last_cuda_error(cudaError_t e);
+}  // namespace mr
+
 #define MR_CUDA_TRY(expr)                                  \
     do {                                                   \
         cudaError_t e_ = (expr);                           \
-        if (e_ != cudaSuccess) return MR_ERR_CUDA;         \
+        if (e_ != cudaSuccess) {                           \
+            mr::set_last_cuda_error(e_);                   \
+            return MR_ERR_CUDA;                            \
+        }                                                  \
     } while (0)
 
 namespace mr {

@@ -47,13 +47,17 @@ constexpr int A_TILE_BYTES = TILE_M * 128;      // 128 rows x 64 values (16 KB)
 constexpr int STAGES = 2;
 constexpr int STAGE_BYTES = 2 * A_TILE_BYTES;   // hi + lo
 constexpr unsigned long long WAIT_NS = 2000000000ull;
+constexpr int EPI_ROW_BYTES = 80;
+constexpr int EPI_STAGE_BYTES = 32 * EPI_ROW_BYTES;
 
 struct RowInfo {                                // one GEMM row (detector row of a view)
     const void* src;                            // first input element of the row
     int pix;                                    // r * C (offset into dark / gain), -1 = padding row
     float b;                                    // FDK row term b0 + r db
     float a0, da, sdd;
-    int pad;
+    float s2b;                                  // sdd^2 + b^2 (vector path)
+    float kx;                                   // x_scale * sdd (* -ln 2 for raw counts; x_scale * (-ln 2) / x_scale without weight)
+    float pad;
 };
 
 struct Args {
@@ -99,19 +103,31 @@ __device__ __forceinline__ unsigned long long global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
+// try_wait that lets the hardware suspend the thread for up to `ns` nanoseconds (it
+// resumes as soon as the phase completes), so waiting warps give their issue slots to
+// the producer warps instead of spinning.
+__device__ __forceinline__ bool bar_try_sleep(uint64_t* b, uint32_t parity, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(b)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
 // Bounded wait: false if another role aborted or this wait exceeded WAIT_NS (then it
 // raises the abort flag and reports MR_ERR_TIMEOUT).
 __device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag, int* status) {
+    if (bar_try(b, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (uint32_t it = 0;; ++it) {
-        if (bar_try(b, parity)) return true;
-        if ((it & 63u) == 63u) {
-            if (*abort_flag) return false;
-            if (global_ns() - t0 > WAIT_NS) {
-                *abort_flag = 1;
-                if (status) atomicExch(status, MR_ERR_TIMEOUT);
-                return false;
-            }
+        if (bar_try_sleep(b, parity, 1000u)) return true;
+        if (*abort_flag) return false;
+        if ((it & 15u) == 15u && global_ns() - t0 > WAIT_NS) {
+            *abort_flag = 1;
+            if (status) atomicExch(status, MR_ERR_TIMEOUT);
+            return false;
         }
     }
 }
@@ -159,6 +175,19 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
 #pragma unroll
     for (int e = 0; e < 32; ++e) v[e] = __uint_as_float(r[e]);
 }
+// Read-only global loads that stay where they are written: the prefetch of the next
+// K-block must be in flight while the current one is converted, and a plain load may be
+// sunk by the compiler to its first use.
+__device__ __forceinline__ uint32_t ldg_u32_now(const void* p) {
+    uint32_t v;
+    asm volatile("ld.global.nc.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float2 ldg_f2_now(const void* p) {
+    float2 v;
+    asm volatile("ld.global.nc.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    return v;
+}
 
 // Byte offset of element (row, k) (k even: a pair of 16-bit values) in a SWIZZLE_128B
 // K-major tile: 16-byte chunk index XOR (row mod 8) inside each 128-byte row.
@@ -167,11 +196,13 @@ __device__ __forceinline__ uint32_t swz(int row, int k) {
 }
 
 // x -> (hi, lo) 16-bit parts, two columns packed per 32-bit word.
-template <bool F16>
+template <bool F16, bool CLAMP = true>
 __device__ __forceinline__ void split2(float2 x, uint32_t& hi, uint32_t& lo) {
     if (F16) {
-        x.x = fminf(fmaxf(x.x, -65504.f), 65504.f);     // finite even for out-of-range inputs
-        x.y = fminf(fmaxf(x.y, -65504.f), 65504.f);
+        if (CLAMP) {
+            x.x = fminf(fmaxf(x.x, -65504.f), 65504.f);     // finite even for out-of-range inputs
+            x.y = fminf(fmaxf(x.y, -65504.f), 65504.f);
+        }
         const __half2 h = __floats2half2_rn(x.x, x.y);
         const float2 hf = __half22float2(h);
         const __half2 l = __floats2half2_rn(x.x - hf.x, x.y - hf.y);
@@ -258,6 +289,11 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
     uint64_t* drain = tfull + 2;                // every issued MMA has completed
     volatile int* abort_flag = reinterpret_cast<volatile int*>(drain + 1);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1) + 1;
+    // epilogue staging, per epilogue warp: 32 rows x 80 bytes (64 bytes of values + 16 of
+    // padding: conflict-free both when a lane writes its row and when 8 rows are read out
+    // for coalesced global stores) and the 32 rows' destinations
+    unsigned char* epi_stage = reinterpret_cast<unsigned char*>(drain + 2);
+    unsigned char** epi_rowp = reinterpret_cast<unsigned char**>(epi_stage + EPI_WARPS * EPI_STAGE_BYTES);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -308,10 +344,10 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
             const int r = (int)(t % A.rows);
             const int vb = (int)(t / A.rows);
             __syncwarp();                                               // previous tile's rows read
+            RowInfo ri{};
+            ri.pix = -1;
             if (lane < RPW) {
                 const int v = vb * TILE_M + pw * RPW + lane;
-                RowInfo ri{};
-                ri.pix = -1;
                 if (v < A.k) {
                     const mr_filter_view fv = A.views[v];
                     const int rr = (RAW && A.flip) ? (A.rows - 1 - r) : r;
@@ -323,10 +359,20 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                     ri.a0 = fv.a0;
                     ri.da = fv.da;
                     ri.b = fmaf((float)r, fv.db, fv.b0);
+                    ri.s2b = fmaf(ri.b, ri.b, fv.sdd * fv.sdd);
+                    // x = lg2(t) * (-ln 2) [raw] * sdd / sqrt(sdd^2 + a^2 + b^2) [cone] * x_scale
+                    ri.kx = (RAW ? -0.69314718056f : 1.f) * A.x_scale * (fv.sdd != 0.f ? fv.sdd : 1.f);
                 }
                 my_rows[lane] = ri;
             }
             __syncwarp();
+            // views of one orbit usually share their FDK constants: then the cosine weight of
+            // a column is the same for all of this warp's rows and is computed once per block
+            const float u_a0 = __shfl_sync(0xffffffffu, ri.a0, 0), u_da = __shfl_sync(0xffffffffu, ri.da, 0);
+            const float u_s2b = __shfl_sync(0xffffffffu, ri.s2b, 0), u_kx = __shfl_sync(0xffffffffu, ri.kx, 0);
+            const float u_sdd = __shfl_sync(0xffffffffu, ri.sdd, 0);
+            const bool uni = __all_sync(0xffffffffu, ri.pix < 0 || (ri.a0 == u_a0 && ri.da == u_da && ri.s2b == u_s2b &&
+                                                                    ri.kx == u_kx && ri.sdd == u_sdd));
             if (fast) {
                 // software pipeline: the loads of K-block I + 1 are in flight while block I
                 // is converted, so each warp keeps 16 rows x 2 blocks of requests outstanding
@@ -343,17 +389,17 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                         const bool live = cin && my_rows[i].pix >= 0;
                         if (RAW) {
                             uint32_t w = 0u;
-                            if (live) w = __ldg(reinterpret_cast<const unsigned int*>(static_cast<const uint16_t*>(src) + c));
+                            if (live) w = ldg_u32_now(static_cast<const uint16_t*>(src) + c);
                             reinterpret_cast<uint32_t*>(buf)[i] = w;
                         } else {
                             float2 w = make_float2(0.f, 0.f);
-                            if (live) w = __ldg(reinterpret_cast<const float2*>(static_cast<const float*>(src) + c));
+                            if (live) w = ldg_f2_now(static_cast<const float*>(src) + c);
                             reinterpret_cast<float2*>(buf)[i] = w;
                         }
                     }
                     if (RAW && cin) {
-                        dk = __ldg(reinterpret_cast<const float2*>(A.dark + r * A.cols + c));
-                        gn = __ldg(reinterpret_cast<const float2*>(A.gain + r * A.cols + c));
+                        dk = ldg_f2_now(A.dark + r * A.cols + c);       // converted to -dark gain at use
+                        gn = ldg_f2_now(A.gain + r * A.cols + c);
                     }
                 };
                 issue(0, cur, dk_c, gn_c);
@@ -370,6 +416,13 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                     const int c = 64 * I + 2 * lane;
                     const bool cin = c < A.cols;
                     const float fc1 = (float)c, fc2 = (float)(c + 1);
+                    const float2 nd = make_float2(-dk_c.x * gn_c.x, -dk_c.y * gn_c.y);   // t = s gain - dark gain
+                    float k1u = u_kx, k2u = u_kx;
+                    if (uni && u_sdd != 0.f) {
+                        const float a1 = fmaf(fc1, u_da, u_a0), a2 = fmaf(fc2, u_da, u_a0);
+                        k1u *= rsqrtf(fmaf(a1, a1, u_s2b));
+                        k2u *= rsqrtf(fmaf(a2, a2, u_s2b));
+                    }
 #pragma unroll
                     for (int i = 0; i < RPW; ++i) {
                         const RowInfo ri = my_rows[i];
@@ -377,21 +430,27 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                         if (cin && ri.pix >= 0) {
                             if (RAW) {
                                 const uint32_t w = reinterpret_cast<const uint32_t*>(cur)[i];
-                                x.x = -__logf(fmaxf(((float)(w & 0xFFFFu) - dk_c.x) * gn_c.x, 1e-3f));
-                                x.y = -__logf(fmaxf(((float)(w >> 16) - dk_c.y) * gn_c.y, 1e-3f));
+                                x.x = __log2f(fmaxf(fmaf((float)(w & 0xFFFFu), gn_c.x, nd.x), 1e-3f));
+                                x.y = __log2f(fmaxf(fmaf((float)(w >> 16), gn_c.y, nd.y), 1e-3f));
                             } else {
                                 x = reinterpret_cast<const float2*>(cur)[i];
                             }
-                            if (ri.sdd != 0.f) {
-                                const float a1 = fmaf(fc1, ri.da, ri.a0), a2 = fmaf(fc2, ri.da, ri.a0);
-                                x.x *= ri.sdd * rsqrtf(fmaf(ri.b, ri.b, fmaf(ri.sdd, ri.sdd, a1 * a1)));
-                                x.y *= ri.sdd * rsqrtf(fmaf(ri.b, ri.b, fmaf(ri.sdd, ri.sdd, a2 * a2)));
+                            float k1 = k1u, k2 = k2u;
+                            if (!uni) {
+                                k1 = ri.kx;
+                                k2 = ri.kx;
+                                if (ri.sdd != 0.f) {
+                                    const float a1 = fmaf(fc1, ri.da, ri.a0), a2 = fmaf(fc2, ri.da, ri.a0);
+                                    k1 *= rsqrtf(fmaf(a1, a1, ri.s2b));
+                                    k2 *= rsqrtf(fmaf(a2, a2, ri.s2b));
+                                }
                             }
-                            x.x *= A.x_scale;
-                            x.y *= A.x_scale;
+                            x.x *= k1;
+                            x.y *= k2;
                         }
                         uint32_t hi, lo;
-                        split2<F16>(x, hi, lo);
+                        // raw counts: |x| < 11.1 * 1024 by construction, no FP16 range clamp needed
+                        split2<F16, !RAW>(x, hi, lo);
                         const uint32_t o = swz(pw * RPW + i, 2 * lane);
                         *reinterpret_cast<uint32_t*>(a_hi + o) = hi;
                         *reinterpret_cast<uint32_t*>(a_lo + o) = lo;
@@ -513,40 +572,63 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                       ((long long)fv.slot * A.slot_stride + (long long)r * A.pitch) * esz;
             }
             const int nch = (A.pitch + 31) / 32;
+            const int nld = (NCOL / 32 < nch) ? NCOL / 32 : nch;         // chunks inside the accumulator
+            const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
+            unsigned char* stg = epi_stage + q * EPI_STAGE_BYTES;
+            unsigned char** rowp = epi_rowp + q * 32;
+            rowp[lane] = live ? out : nullptr;
+            // lane -> (row, 16-byte segment) of the read-out: 8 rows per store instruction
+            const int rd_row = lane >> 2, rd_seg = lane & 3;
             for (int ch = 0; ch < nch; ++ch) {
                 float vv[32];
-                if (32 * ch < NCOL) {                               // warp-uniform: inside the accumulator
-                    tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * ch), vv);
+                if (ch < nld) {                                     // warp-uniform
+                    tmem_ld32(trow + (uint32_t)(32 * ch), vv);
                 } else {
 #pragma unroll
                     for (int e = 0; e < 32; ++e) vv[e] = 0.f;
                 }
-                if (!live) continue;
 #pragma unroll
                 for (int e = 0; e < 32; ++e) vv[e] = (32 * ch + e < A.cols) ? vv[e] * scale : 0.f;
-                if (A.dtype == MR_F32) {
+                // one pass of 32 values (16-bit ring) or two of 16 (FP32): each lane writes its
+                // row's 64 bytes into the staging tile, then the warp stores 8 rows at a time
+                const int passes = A.dtype == MR_F32 ? 2 : 1;
+                for (int h = 0; h < passes; ++h) {
+                    uint4* my = reinterpret_cast<uint4*>(stg + lane * EPI_ROW_BYTES);
+                    if (A.dtype == MR_F32) {
 #pragma unroll
-                    for (int h = 0; h < 8; ++h)
-                        if (32 * ch + 4 * h + 4 <= A.pitch)
-                            *reinterpret_cast<float4*>(out + (32 * ch + 4 * h) * 4) =
-                                make_float4(vv[4 * h], vv[4 * h + 1], vv[4 * h + 2], vv[4 * h + 3]);
-                } else {
-                    uint32_t w[16];
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        if (A.dtype == MR_BF16) {
-                            const __nv_bfloat162 pk = __floats2bfloat162_rn(vv[2 * e], vv[2 * e + 1]);
-                            w[e] = *reinterpret_cast<const uint32_t*>(&pk);
-                        } else {
-                            const __half2 pk = __floats2half2_rn(vv[2 * e], vv[2 * e + 1]);
-                            w[e] = *reinterpret_cast<const uint32_t*>(&pk);
+                        for (int j = 0; j < 4; ++j) {
+                            const int e = 16 * h + 4 * j;
+                            my[j] = make_uint4(__float_as_uint(vv[e]), __float_as_uint(vv[e + 1]),
+                                               __float_as_uint(vv[e + 2]), __float_as_uint(vv[e + 3]));
                         }
-                    }
+                    } else {
+                        uint32_t w[16];
 #pragma unroll
-                    for (int h = 0; h < 4; ++h)
-                        if (32 * ch + 8 * h + 8 <= A.pitch)
-                            *reinterpret_cast<uint4*>(out + (32 * ch + 8 * h) * 2) =
-                                make_uint4(w[4 * h], w[4 * h + 1], w[4 * h + 2], w[4 * h + 3]);
+                        for (int e = 0; e < 16; ++e) {
+                            if (A.dtype == MR_BF16) {
+                                const __nv_bfloat162 pk = __floats2bfloat162_rn(vv[2 * e], vv[2 * e + 1]);
+                                w[e] = *reinterpret_cast<const uint32_t*>(&pk);
+                            } else {
+                                const __half2 pk = __floats2half2_rn(vv[2 * e], vv[2 * e + 1]);
+                                w[e] = *reinterpret_cast<const uint32_t*>(&pk);
+                            }
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) my[j] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
+                    }
+                    __syncwarp();
+                    const int esz = A.dtype == MR_F32 ? 4 : 2;
+                    const int col = 32 * ch + (A.dtype == MR_F32 ? 16 * h + 4 * rd_seg : 8 * rd_seg);
+                    const int per = 16 / esz;                       // elements per 16-byte segment
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int row = 8 * k + rd_row;
+                        unsigned char* dst = rowp[row];
+                        if (dst != nullptr && col + per <= A.pitch)
+                            *reinterpret_cast<uint4*>(dst + col * esz) =
+                                *reinterpret_cast<const uint4*>(stg + row * EPI_ROW_BYTES + 16 * rd_seg);
+                    }
+                    __syncwarp();
                 }
             }
             fence_before();
@@ -564,7 +646,7 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
 
 inline size_t smem_bytes(int kb) {
     return 1024 + (size_t)(2 * kb - 1 + 3) * BLOCK_BYTES + (size_t)STAGES * STAGE_BYTES + TILE_M * sizeof(RowInfo) +
-           (2 * STAGES + 3) * sizeof(uint64_t) + 16;
+           (2 * STAGES + 3) * sizeof(uint64_t) + 16 + EPI_WARPS * (EPI_STAGE_BYTES + 32 * sizeof(void*));
 }
 
 template <bool RAW>
