@@ -373,27 +373,31 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
             const float u_sdd = __shfl_sync(0xffffffffu, ri.sdd, 0);
             const bool uni = __all_sync(0xffffffffu, ri.pix < 0 || (ri.a0 == u_a0 && ri.da == u_da && ri.s2b == u_s2b &&
                                                                     ri.kx == u_kx && ri.sdd == u_sdd));
+            // this warp's rows are consecutive views: row i starts at row 0's input + i * s_view
+            const uint32_t vmask = __ballot_sync(0xffffffffu, lane < RPW && ri.pix >= 0);
+            const unsigned long long src0 = __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(ri.src), 0);
+            const long long vstride = A.s_view * (RAW ? 2 : 4);          // bytes between views
             if (fast) {
-                // software pipeline: the loads of K-block I + 1 are in flight while block I
-                // is converted, so each warp keeps 16 rows x 2 blocks of requests outstanding
-                Pair cur[RPW], nxt[RPW];
+                // software pipeline: the loads of K-blocks I + 1 and I + 2 are in flight while
+                // block I is converted (16 rows x 3 blocks of requests per warp)
+                Pair cur[RPW], n1[RPW], n2[RPW];
 #pragma unroll
-                for (int i = 0; i < RPW; ++i) nxt[i] = Pair{};
-                float2 dk_c = make_float2(0.f, 0.f), gn_c = dk_c, dk_n = dk_c, gn_n = dk_c;
+                for (int i = 0; i < RPW; ++i) n1[i] = n2[i] = Pair{};
+                float2 dk_c = make_float2(0.f, 0.f), gn_c = dk_c, dk_1 = dk_c, gn_1 = dk_c, dk_2 = dk_c, gn_2 = dk_c;
                 auto issue = [&](int I, Pair* buf, float2& dk, float2& gn) {
                     const int c = 64 * I + 2 * lane;
                     const bool cin = c < A.cols;
 #pragma unroll
                     for (int i = 0; i < RPW; ++i) {
-                        const void* src = my_rows[i].src;
-                        const bool live = cin && my_rows[i].pix >= 0;
+                        const unsigned char* src = reinterpret_cast<const unsigned char*>(src0) + i * vstride;
+                        const bool live = cin && ((vmask >> i) & 1u);
                         if (RAW) {
                             uint32_t w = 0u;
-                            if (live) w = ldg_u32_now(static_cast<const uint16_t*>(src) + c);
+                            if (live) w = ldg_u32_now(src + 2 * c);
                             reinterpret_cast<uint32_t*>(buf)[i] = w;
                         } else {
                             float2 w = make_float2(0.f, 0.f);
-                            if (live) w = ldg_f2_now(static_cast<const float*>(src) + c);
+                            if (live) w = ldg_f2_now(src + 4 * c);
                             reinterpret_cast<float2*>(buf)[i] = w;
                         }
                     }
@@ -403,8 +407,9 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                     }
                 };
                 issue(0, cur, dk_c, gn_c);
+                if (KB > 1) issue(1, n1, dk_1, gn_1);
                 for (int I = 0; I < KB; ++I) {
-                    if (I + 1 < KB) issue(I + 1, nxt, dk_n, gn_n);
+                    if (I + 2 < KB) issue(I + 2, n2, dk_2, gn_2);
                     const uint32_t u = (uint32_t)(it * KB + I);
                     const int s = (int)(u & 1u);
                     if (u >= 2 && !bar_wait(&empty[s], ((u >> 1) & 1u) ^ 1u, abort_flag, A.status)) {
@@ -425,9 +430,8 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                     }
 #pragma unroll
                     for (int i = 0; i < RPW; ++i) {
-                        const RowInfo ri = my_rows[i];
                         float2 x = make_float2(0.f, 0.f);
-                        if (cin && ri.pix >= 0) {
+                        if (cin && ((vmask >> i) & 1u)) {
                             if (RAW) {
                                 const uint32_t w = reinterpret_cast<const uint32_t*>(cur)[i];
                                 x.x = __log2f(fmaxf(fmaf((float)(w & 0xFFFFu), gn_c.x, nd.x), 1e-3f));
@@ -437,6 +441,7 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                             }
                             float k1 = k1u, k2 = k2u;
                             if (!uni) {
+                                const RowInfo ri = my_rows[i];
                                 k1 = ri.kx;
                                 k2 = ri.kx;
                                 if (ri.sdd != 0.f) {
@@ -459,9 +464,14 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                     __syncwarp();
                     if (lane == 0) bar_arrive(&full[s]);
 #pragma unroll
-                    for (int i = 0; i < RPW; ++i) cur[i] = nxt[i];
-                    dk_c = dk_n;
-                    gn_c = gn_n;
+                    for (int i = 0; i < RPW; ++i) {
+                        cur[i] = n1[i];
+                        n1[i] = n2[i];
+                    }
+                    dk_c = dk_1;
+                    gn_c = gn_1;
+                    dk_1 = dk_2;
+                    gn_1 = gn_2;
                 }
             } else {
                 // general path (binning, unaligned rows, odd widths): element loads
