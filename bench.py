@@ -419,6 +419,10 @@ def bp_only_and_latency(args, dev, geom, raw_dev, flats, darks, reqs, updates, r
     rec_bf16.add_raw_projections(idx, raw_dev)
     tbf = timed(lambda: rec_bf16.reconstruct_planes_tensor(reqs), rec_bf16.stream)
     t32b = timed(lambda: rec32.reconstruct_planes_tensor(reqs), rec32.stream)
+    # the plain FP32 GPU path: direct global gathers (mr_backproject), one request per launch
+    rec32.bp_kernel = "plain"
+    t32p = timed(lambda: [rec32.reconstruct_planes_tensor([r]) for r in reqs], rec32.stream)
+    rec32.bp_kernel = "staged"
     # per-request latency of the 3-slice batch through the public API (host wall clock,
     # includes descriptor upload and the D2H of the images)
     lat = []
@@ -433,7 +437,9 @@ def bp_only_and_latency(args, dev, geom, raw_dev, flats, darks, reqs, updates, r
         "bp_only": {"bf16_batched_updates_per_s": updates / tbf,
                     "fp32_batched_updates_per_s": updates / t32b,
                     "fp32_one_request_per_launch_updates_per_s": updates / t32,
-                    "bf16_batched_vs_fp32_per_request": t32 / tbf},
+                    "fp32_plain_one_request_per_launch_updates_per_s": updates / t32p,
+                    "bf16_batched_vs_fp32_per_request": t32 / tbf,
+                    "bf16_batched_vs_plain_fp32_per_request": t32p / tbf},
         "latency_ms_3x512_batch": {"p50": float(np.percentile(lat, 50)),
                                    "p99": float(np.percentile(lat, 99)), "samples": len(lat)},
         "_images": imgs,
