@@ -431,8 +431,8 @@ def bp_only_and_latency(args, dev, geom, raw_dev, flats, darks, reqs, updates, r
         rec_bf16.reconstruct_planes(reqs)
         if i >= 5:
             lat.append((time.perf_counter() - t0) * 1e3)
-    imgs = {"bf16": [x.cpu().numpy() for x in rec_bf16.reconstruct_planes_tensor(reqs)],
-            "fp32": [x.cpu().numpy() for x in rec32.reconstruct_planes_tensor(reqs)]}
+    imgs = {f"bf16_store_{rec_bf16.filter_method}_filter": [x.cpu().numpy() for x in rec_bf16.reconstruct_planes_tensor(reqs)],
+            "fp32_store_fft_filter": [x.cpu().numpy() for x in rec32.reconstruct_planes_tensor(reqs)]}
     return {
         "bp_only": {"bf16_batched_updates_per_s": updates / tbf,
                     "fp32_batched_updates_per_s": updates / t32b,
@@ -581,7 +581,7 @@ def main():
     ap.add_argument("--store", choices=("fp32", "bf16", "fp16"), default="bf16")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / accuracy leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the live-scan serving simulation")
-    ap.add_argument("--filter", choices=("fft", "tc", "tc-bf16"), default="fft",
+    ap.add_argument("--filter", choices=("fft", "tc", "tc-bf16"), default="tc",
                     help="row filter: shared-memory FFT or tensor-core Toeplitz GEMM (split FP16 / BF16)")
     args = ap.parse_args()
     if args.warmup < 3:
