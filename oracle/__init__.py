@@ -10,6 +10,7 @@ function by function - each function cites the reference file:line it follows:
   geometry.py geometry.py:60-72, recon.py:70-82 and 225-283 plane helpers, stream.py order
   phantom.py  phantom.py analytic ellipsoid projector (fixture generator)
   recon.py    SliceReconstructor pipeline (recon.py:289-519) at FP32-store / FP64
+  ls.py       few-view least-squares slice refinement (no reference counterpart)
 Parity of this restatement is pinned against golden vectors produced by the reference
 itself (tests/golden/make_golden.py, fixtures in tests/golden/*.npz).
 """

@@ -33,9 +33,12 @@ class BackprojectOp:
     grids   : numpy GRID_DTYPE records; outputs are laid out by their out_offset/strides
     n_out   : length of the flat output
     n_views : views used (default: all records in `views`)
+    scale   : factor of the sum over views (default pi / n_views, the FBP scale; 1 gives the
+              plain back-projection A^T of the matched forward projector A = B^T)
     """
 
-    def __init__(self, views, kind, rows, cols, grids, n_out, n_views=None):
+    def __init__(self, views, kind, rows, cols, grids, n_out, n_views=None, scale=None):
+        self.scale = scale              # None: the FBP scale pi / n_views; else this factor
         self.views = views
         self.kind = kind
         self.rows, self.cols = int(rows), int(cols)
@@ -53,7 +56,10 @@ class BackprojectOp:
         else:
             g["tilt_cos"], g["tilt_sin"] = 0.0, 0.0
         g["n_views"] = self.n_views
-        g["scale"] = math.pi / self.n_views if self.n_views else 0.0
+        if self.scale is not None:
+            g["scale"] = self.scale
+        else:
+            g["scale"] = math.pi / self.n_views if self.n_views else 0.0
         return g
 
     def _ring(self, q):

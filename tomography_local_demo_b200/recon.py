@@ -478,6 +478,8 @@ class SliceReconstructor:
     tilt     : detector tilt correction in degrees (rotates each projection).
     store    : filtered-view storage, "fp32" (default), "bf16" or "fp16".
     device   : CUDA device (default: the current one).
+    keep_projections : also keep the unfiltered (pre-processed) line integrals of every
+               received view on the device (FP32, the ring's layout), for refine_slice_ls.
     filter   : "fft" (default; shared-memory FFT, FP32), "tc" (Toeplitz GEMM on the tensor
                cores, split FP16 operands, FP32 accumulation; rows <= 512 columns) or
                "tc-bf16" (the same with split BF16 operands, ~100x less precise on
@@ -487,7 +489,8 @@ class SliceReconstructor:
     """
 
     def __init__(self, proj=None, geom=None, window="shepp-logan", backend="auto",
-                 gaussian=0.0, tilt=0.0, verbose=True, store="fp32", device=None, filter="fft"):
+                 gaussian=0.0, tilt=0.0, verbose=True, store="fp32", device=None, filter="fft",
+                 keep_projections=False):
         if geom is None:
             raise ValueError("geometry is required")
         if store not in _STORE_DTYPES:
@@ -545,6 +548,10 @@ class SliceReconstructor:
             self._views_dev = torch.zeros(self.n_total * N.VIEW_DTYPE.itemsize, dtype=torch.uint8,
                                           device=self.device)
         self._ring_c = _ring_struct(self._ring, self._dtype_code, self._kind_code, R, C)
+        self._proj = None               # unfiltered line integrals [n_total, R, pitch] (keep_projections)
+        if keep_projections:
+            with torch.cuda.device(self.device):
+                self._proj = torch.zeros((self.n_total, R, self._pitch), dtype=torch.float32, device=self.device)
         self._ingest_event = None
         self._raw_dev = None            # device staging of host raw counts (grows on demand)
         self._raw_pinned = []           # pinned staging of pageable raw counts, one per chunk slot
@@ -615,6 +622,8 @@ class SliceReconstructor:
             with torch.cuda.device(self.device), torch.cuda.stream(self.ingest_stream):
                 x = _to_device_tensor(block, self.device, torch.float32)      # [R, k, C]
                 x, s_view, s_row = preprocess.apply_device(x, self.gaussian, self.tilt)
+                if self._proj is not None:
+                    self._proj[n0:n0 + k, :, :C] = torch.as_strided(x, (k, R, C), (s_view, s_row, 1))
                 fv = _struct_tensor(self._filter_views(indices, slots), self.device)
                 filter_block_device(x, s_view, s_row, k, fv, self._tables, self._ring_c,
                                     self.ingest_stream, self.filter_method, self._status)
@@ -695,6 +704,8 @@ class SliceReconstructor:
             slots = np.arange(n0, n0 + k)
             fv_host = self._filter_views(indices, slots)
             on_device = isinstance(raw, torch.Tensor) and raw.is_cuda
+            if self._proj is not None:
+                self._keep_raw_line_integrals(raw, n0, k)
             with torch.cuda.device(self.device), torch.cuda.stream(self.ingest_stream):
                 fv_pinned = torch.from_numpy(np.ascontiguousarray(fv_host).view(np.uint8).copy()).pin_memory()
                 fv = fv_pinned.to(self.device, non_blocking=True)
@@ -709,6 +720,84 @@ class SliceReconstructor:
                     self._ingest_host(raw, k, fv)
                 ev = torch.cuda.Event()
             return self._admit(indices, slots, ev)
+
+    def _keep_raw_line_integrals(self, raw, n0, k):
+        """-log(max((binned counts - dark) * gain, 1e-3)) of k raw views into the kept
+        projections (the correction of the fused ingest, without its filter)."""
+        b, R, C = self._raw_bin, self.geom.rows, self.geom.cols
+        with torch.cuda.device(self.device), torch.cuda.stream(self.ingest_stream):
+            t = raw if isinstance(raw, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(raw).view(np.int16))
+            t = t.to(self.device, non_blocking=True)
+            t = (t.view(torch.int16).to(torch.int32) & 0xFFFF).to(torch.float32)       # uint16 counts
+            t = t[:, :R * b, :C * b].reshape(k, R, b, C, b).mean(dim=(2, 4))
+            if self._raw_flip:
+                t = torch.flip(t, dims=[1])
+            x = -torch.log(torch.clamp((t - self._dark) * self._gain, min=1e-3))
+            self._proj[n0:n0 + k, :, :C] = x
+
+    def refine_slice_ls(self, origin=(0.0, 0.0, 0.0), normal=(0.0, 0.0, 1.0), n=256, size=None, zoom=1.0,
+                        center=None, iters=10):
+        """Least-squares refinement of a slice from the views received so far (few views
+        during a live scan): CGLS on min ||A x - c p||^2 over the slice's in-box samples,
+        started from the FBP slice. A is the matched forward projector of the slice
+        samples (the exact transpose of the bilinear back-projection, mr_project_adjoint),
+        A^T the plain back-projection, p the kept unfiltered line integrals
+        (keep_projections=True), c the least-squares scale that makes the FBP slice x0 fit
+        A x0 ~ c p (the sample-spacing factor of the discretisation).
+        The slice is modelled as the only object on its rays, which is exact for axial
+        slices of a parallel-beam scan placed on a detector row (each detector row sees one
+        axial slice) and an approximation otherwise (cone beam near the mid-plane).
+        Returns (img [n, n] f64, residual norms per iteration)."""
+        from .autograd import BackprojectOp
+        if self._proj is None:
+            raise RuntimeError("refine_slice_ls needs SliceReconstructor(..., keep_projections=True)")
+        n_views, shift, ev = self._snapshot()
+        if n_views == 0:
+            raise RuntimeError("no projections received yet")
+        grid = plane_grid(self.box, origin, normal, int(n), size, zoom, center, shift)
+        grids = np.zeros(1, dtype=N.GRID_DTYPE)
+        grids[0] = grid
+        R, C = self.geom.rows, self.geom.cols
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            if ev is not None:
+                self.stream.wait_event(ev)
+            op = BackprojectOp(self._views_dev, self._kind_code, R, C, grids, n * n, n_views, scale=1.0)
+            fbp = BackprojectOp(self._views_dev, self._kind_code, R, C, grids, n * n, n_views)
+            x = fbp.forward(self._ring, shift)
+            shape = (n_views, R, self._pitch)
+            # detector pixels the slice reaches with a real weight (FP32 coordinates can put
+            # ~1e-6 of a sample on a neighbouring row): the data term covers only those
+            w1 = op.adjoint(torch.ones(n * n, dtype=torch.float32, device=self.device), shift, 0.0, shape)
+            mask = (w1 > 1e-3 * float(w1.max())).float()
+            A = lambda v: op.adjoint(v, shift, 0.0, shape) * mask         # noqa: E731  samples -> detector
+            AT = lambda r: op.forward(r * mask, shift)                    # noqa: E731  detector -> samples
+            p = self._proj[:n_views]
+            Ax = A(x)
+            pm = p * mask
+            c = float((Ax * pm).sum() / (pm * pm).sum().clamp_min(1e-30))
+            b = c * pm
+            r = b - Ax
+            s = AT(r)
+            d = s.clone()
+            gamma = float((s * s).sum())
+            hist = [float(r.norm())]
+            for _ in range(int(iters)):
+                if gamma <= 0.0:
+                    break
+                q = A(d)
+                qq = float((q * q).sum())
+                if qq <= 0.0:
+                    break
+                alpha = gamma / qq
+                x = x + alpha * d
+                r = r - alpha * q
+                s = AT(r)
+                gamma_new = float((s * s).sum())
+                d = s + (gamma_new / gamma) * d
+                gamma = gamma_new
+                hist.append(float(r.norm()))
+            img = x.view(n, n).double().cpu().numpy()
+        return img, hist
 
     def _ingest_launch(self, x, c0, c1, fv):
         """mr_ingest_u16 of views [c0, c1) of the device raw block x on the ingest stream."""
