@@ -1031,6 +1031,28 @@ class SliceReconstructor:
         _handoff(self.stream, vol)
         return vol, origin, h
 
+    def reconstruct_volume_slab_tensor(self, k0, k1, voxel=None, maxdim=None):
+        """x-planes [k0, k1) of the volume of reconstruct_volume (same frame), as a device
+        tensor [k1 - k0, ny, nz]: the unit of work of a volume sharded over GPUs."""
+        dims, origin, h = self._volume_frame(voxel, maxdim)
+        nx, ny, nz = dims
+        k0, k1 = int(k0), int(k1)
+        if not 0 <= k0 <= k1 <= nx:
+            raise ValueError(f"slab [{k0}, {k1}) outside the volume's {nx} planes")
+        n_views, shift, ev = self._snapshot()
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            slab = torch.empty((k1 - k0, ny, nz), dtype=torch.float32, device=self.device)
+            if n_views == 0 or k1 == k0:
+                slab.zero_()
+            else:
+                g = np.zeros(1, dtype=N.GRID_DTYPE)
+                g[0] = volume_grid_record(origin, h, dims, k0, k1)
+                g["out_offset"] = 0
+                g["cor_shift"] = shift
+                self._run_grids(g, slab.view(-1), n_views, ev)
+        _handoff(self.stream, slab)
+        return slab, origin, h
+
     def reconstruct_volume(self, voxel=None, maxdim=None, chunk=262144, progress=None):
         """Full 3D reconstruction of the volume box on a regular grid.
         Returns (volume [nx, ny, nz] float32, origin (mm), voxel size (mm))."""
