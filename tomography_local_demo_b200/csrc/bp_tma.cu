@@ -8,9 +8,8 @@
 //     detector are zero-filled by the TMA unit, which is exactly the reference's
 //     "bilinear taps outside [0,R)x[0,C) contribute 0";
 //   * a warp-specialised ring of stages: one producer warp computes footprints and issues
-//     the TMA loads, four consumer warps back-project eight samples per thread (one
-//     straight-line block when all of a warp's samples lie in the box); full/empty
-//     mbarriers (bounded waits) are the only synchronisation inside the view loop;
+//     the TMA loads, eight consumer warps back-project; full/empty mbarriers (bounded
+//     waits) are the only synchronisation inside the view loop;
 //   * the consumer loop is predicate-free: floor via a round-down FMA against a magic
 //     constant (FMA pipe only), one unsigned clamp for memory safety, four LDS, lerps;
 //   * footprints that miss the detector entirely are skipped (exactly zero), and the
@@ -30,10 +29,9 @@ namespace cg = cooperative_groups;
 namespace mr {
 
 constexpr int ST_TI = 32, ST_TJ = 32;        // tile (samples) - same tiling as bp.cu
-constexpr int ST_CONSUMERS = 4;               // consumer warps (one 32 x 32 tile)
+constexpr int ST_CONSUMERS = 8;               // consumer warps (one 32 x 32 tile)
 constexpr int ST_THREADS = 32 * (ST_CONSUMERS + 1);   // + one producer warp
-constexpr int ST_PPT = 8;                     // samples per consumer thread (rows i, i+4, ..., i+28)
-constexpr int ST_PV = ST_PPT / 4;             // float4 partial sums per consumer thread
+constexpr int ST_PPT = 4;                     // samples per consumer thread (i, i+4, i+8, i+12)
 constexpr int ST_BOX_H = 8;                   // rows per TMA box
 constexpr int ST_MAX_BOXES = 10;              // <= 80 staged rows per view
 constexpr int ST_CLUSTER = 4;                 // CTAs per tile, each a quarter of the views
@@ -93,12 +91,26 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-// Stored element from shared memory, widened to FP32.
-__device__ __forceinline__ float smem_elem(const float* p) { return *p; }
-__device__ __forceinline__ float smem_elem(const __nv_bfloat16* p) {
-    return __uint_as_float(static_cast<uint32_t>(*reinterpret_cast<const unsigned short*>(p)) << 16);
+template <typename T>
+__device__ __forceinline__ float lds_elem(uint32_t addr);
+template <>
+__device__ __forceinline__ float lds_elem<float>(uint32_t addr) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    return v;
 }
-__device__ __forceinline__ float smem_elem(const __half* p) { return __half2float(*p); }
+template <>
+__device__ __forceinline__ float lds_elem<__nv_bfloat16>(uint32_t addr) {
+    unsigned short u;
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(u) : "r"(addr));
+    return __uint_as_float(static_cast<uint32_t>(u) << 16);
+}
+template <>
+__device__ __forceinline__ float lds_elem<__half>(uint32_t addr) {
+    unsigned short u;
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(u) : "r"(addr));
+    return __half2float(__ushort_as_half(u));
+}
 
 // Global-memory bilinear (fallback for footprints larger than a stage).
 template <typename T>
@@ -208,7 +220,7 @@ __device__ __forceinline__ ViewMeta view_meta(const mr_view& V, const mr_grid& g
 // r-th quarter of the views and rank 0 sums the partials from the others' shared memory
 // (DSMEM) in rank order - deterministic, no atomics, no scratch - and writes the tile.
 template <int KIND, typename T>
-__global__ void __launch_bounds__(ST_THREADS, 4)
+__global__ void __launch_bounds__(ST_THREADS)
 bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__ ring, int R, int C,
                  int pitch, long long slot_stride, const mr_view* __restrict__ views,
                  const mr_grid* __restrict__ grids, const mr_tile* __restrict__ tiles,
@@ -231,7 +243,7 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
     ViewMeta* meta_new = meta_ring + S;                                              // 32
     uint64_t* full = reinterpret_cast<uint64_t*>(meta_new + 32);                    // S
     uint64_t* empty = full + S;                                                      // S
-    float4* partial = reinterpret_cast<float4*>(empty + S);    // ST_PV x consumer threads (cluster sum)
+    float4* partial = reinterpret_cast<float4*>(empty + S);                          // 256 (cluster sum)
     __shared__ mr_grid s_g;
 
     cg::cluster_group cluster = cg::this_cluster();
@@ -298,12 +310,8 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
         const bool tile_live = __syncthreads_or(any) != 0;
         // warp-uniform: an 8x4 sample patch wholly outside the box is not computed
         bool wlive[ST_PPT];
-        bool all_live = true;
 #pragma unroll
-        for (int p = 0; p < ST_PPT; ++p) {
-            wlive[p] = __any_sync(0xffffffffu, inside[p]);
-            all_live = all_live && wlive[p];
-        }
+        for (int p = 0; p < ST_PPT; ++p) wlive[p] = __any_sync(0xffffffffu, inside[p]);
 
         if (producer && tile_live) {
             const int di_max = min(ST_TI, g.n_i - t.i0) - 1;
@@ -351,13 +359,13 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                 const float bv = fmaf(fj, m.cv.z, m.cv.x);
                 const float bw = fmaf(fj, m.cw.z, m.cw.x);
                 if (m.mode == MODE_STAGED) {
-                    const unsigned char* sbase = stages + s * STAGE_BYTES;
+                    const uint32_t base = smem_u32(stages + s * STAGE_BYTES);
                     const uint32_t maxoff = (uint32_t)(m.nbox * BOX_BYTES - (W + 1) * ESZ - ESZ);
                     // byte offset = (bits_r - MAGIC_BITS) * W*ESZ + (bits_c - MAGIC_BITS) * ESZ
                     const uint32_t kofs = (uint32_t)MAGIC_BITS * (uint32_t)(W * ESZ + ESZ);
-                    // plain shared loads (ordered after the stage's full-barrier wait by its
-                    // memory clobber), so the compiler can interleave the samples' gathers
-                    auto sample = [&](int p) {
+#pragma unroll
+                    for (int p = 0; p < ST_PPT; ++p) {
+                        if (!wlive[p]) continue;
                         const float fi = (float)(ty + 4 * p);
                         const float nu = fmaf(fi, m.cu.y, bu);
                         const float nvv = fmaf(fi, m.cv.y, bv);
@@ -377,23 +385,15 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                         uint32_t off = (uint32_t)__float_as_int(yr) * (uint32_t)(W * ESZ) +
                                        (uint32_t)__float_as_int(yc) * (uint32_t)ESZ - kofs;
                         off = min(off, maxoff);
-                        const T* a = reinterpret_cast<const T*>(sbase + off);
-                        const float q00 = smem_elem(a);
-                        const float q01 = smem_elem(a + 1);
-                        const float q10 = smem_elem(a + W);
-                        const float q11 = smem_elem(a + W + 1);
+                        const uint32_t a = base + off;
+                        const float q00 = lds_elem<T>(a);
+                        const float q01 = lds_elem<T>(a + ESZ);
+                        const float q10 = lds_elem<T>(a + W * ESZ);
+                        const float q11 = lds_elem<T>(a + W * ESZ + ESZ);
                         const float ta = fmaf(fc, q01 - q00, q00);
                         const float tb = fmaf(fc, q11 - q10, q10);
                         const float val = fmaf(fr, tb - ta, ta);
                         acc[p] = fmaf(KIND == MR_CONE ? r * r : m.cu.w, val, acc[p]);
-                    };
-                    if (all_live) {                 // warp-uniform: straight-line samples
-#pragma unroll
-                        for (int p = 0; p < ST_PPT; ++p) sample(p);
-                    } else {
-#pragma unroll
-                        for (int p = 0; p < ST_PPT; ++p)
-                            if (wlive[p]) sample(p);
                     }
                 } else if (m.mode == MODE_GLOBAL) {
                     const T* q = ring + (long long)(v_begin + v) * slot_stride;
@@ -419,20 +419,12 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
 
         // ---- cluster reduction of the view-quarter partial sums (rank order), rank 0 writes
         if (csize > 1) {
-            if (!producer) {
-#pragma unroll
-                for (int h = 0; h < ST_PV; ++h)
-                    partial[h * ST_CONSUMERS * 32 + tid] = make_float4(acc[4 * h], acc[4 * h + 1], acc[4 * h + 2], acc[4 * h + 3]);
-            }
+            if (!producer) partial[tid] = make_float4(acc[0], acc[1], acc[2], acc[3]);
             cluster.sync();
             if (crank == 0 && !producer) {
                 for (int r = 1; r < csize; ++r) {
-                    const float4* peer = cluster.map_shared_rank(partial, r);
-#pragma unroll
-                    for (int h = 0; h < ST_PV; ++h) {
-                        const float4 o = peer[h * ST_CONSUMERS * 32 + tid];
-                        acc[4 * h] += o.x; acc[4 * h + 1] += o.y; acc[4 * h + 2] += o.z; acc[4 * h + 3] += o.w;
-                    }
+                    const float4 o = cluster.map_shared_rank(partial, r)[tid];
+                    acc[0] += o.x; acc[1] += o.y; acc[2] += o.z; acc[3] += o.w;
                 }
             }
         }
@@ -493,7 +485,7 @@ static int launch_staged(const mr_ring* ring, const mr_view* views, const mr_gri
     constexpr int S = StageGeom<T>::STAGES;
     const size_t smem = (size_t)S * StageGeom<T>::W * ST_BOX_H * ST_MAX_BOXES * sizeof(T) +
                         (S + 32) * sizeof(ViewMeta) + 2 * S * sizeof(uint64_t) +
-                        ST_CONSUMERS * 32 * ST_PV * sizeof(float4) + 128;
+                        ST_CONSUMERS * 32 * sizeof(float4) + 128;
     auto kern = bp_staged_kernel<KIND, T>;
     MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     cudaLaunchConfig_t cfg = {};
