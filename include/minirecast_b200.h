@@ -72,7 +72,7 @@ typedef struct mr_view {
 /* Sample grid of one reconstruction request. 256 bytes.
  *   p(i,j,k) = origin + i*step_i + j*step_j + k*step_k   (mm, FP32)
  *   out[out_offset + i*out_stride_i + j*out_stride_j + k*out_stride_k]
- *       = scale * sum_{v < n_views} w_v(p) * bilinear(ring[v], row_v(p), col_v(p))
+ *       (+)= scale * sum_{view_begin <= v < view_begin + n_views} w_v(p) * bilinear(ring[v], row_v(p), col_v(p))
  * With MR_GRID_MASK_BOX a sample is written as 0 unless the FP64 point
  *   c + a_j*e_j + a_i*e_i,  a_x = (x - mask_half) * mask_delta
  * lies in the box (|p_x| <= box_x for every axis), evaluated in the rounding order
@@ -105,7 +105,10 @@ typedef struct mr_grid {
     double  mask_half;      /* (n - 1) / 2 */
     double  mask_delta;     /* pixel size */
     double  box[3];         /* half sizes of the volume box */
-    int64_t pad2[2];
+    int32_t view_begin;     /* first slot summed: slots [view_begin, view_begin + n_views) */
+    int32_t accumulate;     /* 0: out = result (0 outside the box); 1: out += result (a
+                               partial sum over a range of views, same scale) */
+    int64_t pad2;
 } mr_grid;
 
 /* One work item of a back-projection launch: a tile of one grid. 16 bytes. */

@@ -201,3 +201,79 @@ def test_staged_kernel_edge_footprints(cuda, store):
         want = oracle_cone(V, stack, pts.reshape(-1, 3)[mask.ravel()], A)
         assert np.all(img[~mask] == 0)
         assert rel_l2(img[mask], want) < 5e-5
+
+
+@pytest.mark.parametrize("kernel", ["staged", "plain", "points"])
+def test_view_ranges_accumulate_to_the_full_sum(cuda, kernel):
+    """mr_grid.view_begin / accumulate: a sub-range of slots alone matches the oracle on
+    those views, and ranges summed in order (the first writes, the rest add) equal the
+    one-launch sum over all views to FP32 rounding, with the same zeros outside the box."""
+    import torch
+    V, q, rows, cols = cone_case(A=45, seed=13)
+    box = og.cone_volume_box(V, rows, cols)
+    ring = DeviceRing(q, R.cone_view_maps(R.cone_constants(V), rows, cols), N.MR_CONE)
+    scale = np.pi / len(V)
+    if kernel == "points":
+        pts = np.random.default_rng(6).uniform(-20, 20, (3001, 3))
+        p_dev = torch.from_numpy(pts.astype(np.float32)).to(ring.dev)
+        g = np.zeros(1, N.GRID_DTYPE)
+        g["n_i"], g["n_j"], g["n_k"] = 1, len(pts), 1
+        g["flags"] = N.MR_GRID_POINTS
+        g["out_stride_j"] = 1
+        g["points"] = p_dev.data_ptr()
+        n_out, kern = len(pts), "plain"
+        mask = np.ones(len(pts), bool)
+    else:
+        g = np.zeros(2, N.GRID_DTYPE)
+        g[0] = R.plane_grid(box, (1, -2, 0.5), (0.3, 0.2, 1.0), 61, None, 1.0, None, 0.4)
+        g[1] = R.plane_grid(box, (0, 3, 1), (1.0, 0.1, 0.2), 47, None, 0.7, None, 0.0)
+        g[1]["out_offset"] = 61 * 61
+        n_out, kern = 61 * 61 + 47 * 47, kernel
+        pts0, m0 = og.slice_points(box, (1, -2, 0.5), (0.3, 0.2, 1.0), 61, None, 1.0, None)
+        mask = np.concatenate([m0.ravel(), og.slice_points(box, (0, 3, 1), (1.0, 0.1, 0.2), 47, None,
+                                                           0.7, None)[1].ravel()])
+    g["scale"] = scale
+    full = g.copy()
+    full["n_views"] = len(V)
+    want = ring.run(full, n_out, kern)
+    # one sub-range alone, against the oracle on those views
+    sub = g.copy()
+    sub["view_begin"], sub["n_views"] = 11, 17
+    got_sub = ring.run(sub, n_out, kern)
+    if kernel == "points":
+        K = of.cone_constants(V[11:28])
+        ref = obp.bp_cone(q[11:28], K["s"], K["d"], K["uu"], K["vv"], K["n"], K["sdd"], K["sod"],
+                          pts, scale)
+        assert rel_l2(got_sub, ref) < 5e-5
+    else:
+        ref = np.zeros(n_out)
+        K = of.cone_constants(V[11:28])
+        pts1 = og.slice_points(box, (0, 3, 1), (1.0, 0.1, 0.2), 47, None, 0.7, None)[0]
+        D0 = K["d"] - 0.4 * K["u"]
+        P0 = pts0.reshape(-1, 3)[m0.ravel()]
+        ref[:61 * 61][m0.ravel()] = obp.bp_cone(q[11:28], K["s"], D0, K["uu"], K["vv"], K["n"], K["sdd"],
+                                                K["sod"], P0, scale)
+        m1 = mask[61 * 61:]
+        ref[61 * 61:][m1] = obp.bp_cone(q[11:28], K["s"], K["d"], K["uu"], K["vv"], K["n"], K["sdd"],
+                                        K["sod"], pts1.reshape(-1, 3)[m1], scale)
+        assert np.all(got_sub[~mask] == 0)
+        assert rel_l2(got_sub[mask], ref[mask]) < 5e-5
+    # a range running past the ring is clamped to its slots: [40, 140) sums slots 40..44
+    over = g.copy()
+    over["view_begin"], over["n_views"] = 40, 100
+    tail = g.copy()
+    tail["view_begin"], tail["n_views"] = 40, 5
+    np.testing.assert_array_equal(ring.run(over, n_out, kern), ring.run(tail, n_out, kern))
+    # ranges summed in order into one buffer
+    out = torch.full((n_out,), float("nan"), dtype=torch.float32, device=ring.dev)
+    status = torch.zeros(1, dtype=torch.int32, device=ring.dev)
+    st = torch.cuda.current_stream()
+    for i, (a, b) in enumerate([(0, 7), (7, 30), (30, 31), (31, 45)]):
+        part = g.copy()
+        part["view_begin"], part["n_views"], part["accumulate"] = a, b - a, int(i > 0)
+        R.backproject_device(ring.c, ring.views, part, out, st, ring.dev, kernel=kern, status=status)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    got = out.cpu().numpy().astype(np.float64)
+    assert np.all(got[~mask] == 0) and np.all(want[~mask] == 0)
+    assert rel_l2(got[mask], want[mask]) < 1e-6

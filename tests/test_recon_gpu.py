@@ -228,5 +228,12 @@ def test_raw_ingest_input_kinds_and_chunked_upload(cuda, kind):
     rec, got, order = ingest(src, 3 * 48 * 72 * 2)                         # 3 views per chunk
     np.testing.assert_array_equal(order, want_order)
     np.testing.assert_array_equal(got, want)
+    # right after a chunked host upload a slice sums the views chunk by chunk (each partial
+    # launch waits only for its chunk): the same result up to the FP32 summation order
     req = dict(origin=(1.0, -2.0, 0.5), normal=(0.3, 0.2, 1.0), n=40)
-    np.testing.assert_array_equal(rec.reconstruct_planes([req])[0], want_rec.reconstruct_planes([req])[0])
+    got_img = rec.reconstruct_planes([req])[0]
+    want_img = want_rec.reconstruct_planes([req])[0]
+    np.testing.assert_array_equal(got_img == 0, want_img == 0)
+    assert rel_l2(got_img, want_img) < 1e-6
+    if kind != "cuda":
+        assert len(rec._chunk_marks) >= 2            # the split path was taken

@@ -33,7 +33,8 @@ GRID_DTYPE = np.dtype([("origin", "<f4", 3), ("step_i", "<f4", 3), ("step_j", "<
                        ("out_stride_i", "<i8"), ("out_stride_j", "<i8"), ("out_stride_k", "<i8"),
                        ("points", "<u8"), ("tilt_cos", "<f4"), ("tilt_sin", "<f4"), ("mask_c", "<f8", 3),
                        ("mask_ej", "<f8", 3), ("mask_ei", "<f8", 3), ("mask_half", "<f8"),
-                       ("mask_delta", "<f8"), ("box", "<f8", 3), ("pad2", "<i8", 2)], align=True)
+                       ("mask_delta", "<f8"), ("box", "<f8", 3), ("view_begin", "<i4"), ("accumulate", "<i4"),
+                       ("pad2", "<i8")], align=True)
 TILE_DTYPE = np.dtype([("grid", "<i4"), ("i0", "<i4"), ("j0", "<i4"), ("k", "<i4")], align=True)
 FILTER_VIEW_DTYPE = np.dtype([("a0", "<f4"), ("da", "<f4"), ("b0", "<f4"), ("db", "<f4"),
                               ("sdd", "<f4"), ("gain", "<f4"), ("out_scale", "<f4"),

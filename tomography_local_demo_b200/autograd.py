@@ -56,6 +56,7 @@ class BackprojectOp:
         else:
             g["tilt_cos"], g["tilt_sin"] = 0.0, 0.0
         g["n_views"] = self.n_views
+        g["view_begin"], g["accumulate"] = 0, 0      # slots [0, n_views), written (not added)
         if self.scale is not None:
             g["scale"] = self.scale
         else:

@@ -68,8 +68,8 @@ __device__ __forceinline__ float dot3(const float* a, float x, float y, float z)
 
 template <int KIND, typename T>
 __global__ void __launch_bounds__(BP_THREADS)
-bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_stride,
-          const mr_view* __restrict__ views, const mr_grid* __restrict__ grids,
+bp_kernel(const T* __restrict__ ring_all, int R, int C, int pitch, long long slot_stride, int n_slots,
+          const mr_view* __restrict__ views_all, const mr_grid* __restrict__ grids,
           const mr_tile* __restrict__ tiles, float* __restrict__ out) {
     __shared__ float4 s_u[BP_VCH], s_v[BP_VCH], s_w[BP_VCH];
     __shared__ float s_q[BP_VCH];
@@ -86,8 +86,12 @@ bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_st
         reinterpret_cast<int*>(&s_g)[tid] = reinterpret_cast<const int*>(grids + t.grid)[tid];
     __syncthreads();
     const mr_grid& g = s_g;
-    const int nv = g.n_views;
     const bool points = (g.flags & MR_GRID_POINTS) != 0;
+    // the grid sums slots [first, first + nv)
+    int first, nv;
+    grid_view_range(g.view_begin, g.n_views, n_slots, &first, &nv);
+    const mr_view* __restrict__ views = views_all + first;
+    const T* __restrict__ ring = ring_all + (long long)first * slot_stride;
 
     float acc[BP_PPT];
 #pragma unroll
@@ -165,7 +169,8 @@ bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_st
             if (i < g.n_i && j < g.n_j) {
                 const long long o = g.out_offset + (long long)i * g.out_stride_i +
                                     (long long)j * g.out_stride_j + (long long)t.k * g.out_stride_k;
-                out[o] = inside[p] ? acc[p] * g.scale : 0.f;
+                const float val = inside[p] ? acc[p] * g.scale : 0.f;
+                out[o] = g.accumulate ? out[o] + val : val;
             }
         }
     } else {
@@ -219,7 +224,10 @@ bp_kernel(const T* __restrict__ ring, int R, int C, int pitch, long long slot_st
 #pragma unroll
         for (int p = 0; p < BP_PPT; ++p) {
             const int j = t.j0 + tid + BP_THREADS * p;
-            if (ok[p]) out[g.out_offset + (long long)j * g.out_stride_j] = acc[p] * g.scale;
+            if (ok[p]) {
+                float* o = out + g.out_offset + (long long)j * g.out_stride_j;
+                *o = g.accumulate ? *o + acc[p] * g.scale : acc[p] * g.scale;
+            }
         }
     }
 }
@@ -234,7 +242,7 @@ static int launch_bp(const mr_ring* ring, const mr_view* views, const mr_grid* g
         const int64_t n = (n_tiles - t0) < max_chunk ? (n_tiles - t0) : max_chunk;
         bp_kernel<KIND, T><<<(unsigned)n, block, 0, st>>>(
             static_cast<const T*>(ring->data), ring->rows, ring->cols, ring->col_pitch,
-            (long long)ring->slot_stride, views, grids, tiles + t0, out);
+            (long long)ring->slot_stride, (int)ring->n_slots, views, grids, tiles + t0, out);
     }
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;

@@ -28,7 +28,8 @@ enum : int { GRAD_ADJOINT = 0, GRAD_GEOM = 1, GRAD_FORWARD = 2 };
 template <int KIND, int MODE, typename T>
 __global__ void __launch_bounds__(GR_THREADS)
 bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int C, int pitch,
-               long long slot_stride, const mr_view* __restrict__ views, const mr_grid* __restrict__ grids,
+               long long slot_stride, int n_slots, const mr_view* __restrict__ views,
+               const mr_grid* __restrict__ grids,
                const mr_tile* __restrict__ tiles, const float* __restrict__ gout, double* __restrict__ dgeom) {
     __shared__ float4 s_u[GR_VCH], s_v[GR_VCH], s_w[GR_VCH];
     __shared__ float s_q[GR_VCH], s_uv[GR_VCH];
@@ -94,12 +95,13 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
     const float shift = g.cor_shift;
     const float cc = 0.5f * (float)(C - 1), cr = 0.5f * (float)(R - 1);
     float ds = 0.f, dt = 0.f;
-    const int nv = g.n_views;
+    int first, nv;                      // slots [first, first + nv)
+    grid_view_range(g.view_begin, g.n_views, n_slots, &first, &nv);
     for (int v0 = 0; v0 < nv; v0 += GR_VCH) {
         const int nch = min(GR_VCH, nv - v0);
         __syncthreads();
         if (tid < nch) {
-            const mr_view V = views[v0 + tid];
+            const mr_view V = views[first + v0 + tid];
             float pu[4], pv[4];
             view_map(V, g, R, C, pu, pv);
             s_u[tid] = make_float4(pu[0], pu[1], pu[2], pu[3]);
@@ -112,7 +114,7 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
         for (int vv = 0; vv < nch; ++vv) {
             const float4 cu = s_u[vv], cv = s_v[vv], cw = s_w[vv];
             const float qs = s_q[vv], uv = s_uv[vv];
-            const long long slot = (long long)(v0 + vv) * slot_stride;
+            const long long slot = (long long)(first + v0 + vv) * slot_stride;
 #pragma unroll
             for (int p = 0; p < GR_PPT; ++p) {
                 if (MODE == GRAD_FORWARD ? !live[p] : gp[p] == 0.f) continue;
@@ -168,7 +170,10 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
         for (int p = 0; p < GR_PPT; ++p) {
             const bool ok = pts ? (t.j0 + tid + GR_THREADS * p < g.n_j)
                                 : (t.i0 + ty + 4 * p < g.n_i && t.j0 + tx < g.n_j);
-            if (ok) gring[oidx[p]] = live[p] ? acc[p] * g.scale : 0.f;
+            if (ok) {
+                const float val = live[p] ? acc[p] * g.scale : 0.f;
+                gring[oidx[p]] = g.accumulate ? gring[oidx[p]] + val : val;
+            }
         }
     }
     if (MODE == GRAD_GEOM) {
@@ -196,7 +201,7 @@ static int launch_grad(const mr_ring* ring, float* gring, const mr_view* views, 
         const int64_t n = (n_tiles - t0) < max_chunk ? (n_tiles - t0) : max_chunk;
         bp_grad_kernel<KIND, MODE, T><<<(unsigned)n, GR_THREADS, 0, st>>>(
             static_cast<const T*>(ring->data), gring, ring->rows, ring->cols, ring->col_pitch,
-            (long long)ring->slot_stride, views, grids, tiles + t0, gout, dgeom);
+            (long long)ring->slot_stride, (int)ring->n_slots, views, grids, tiles + t0, gout, dgeom);
     }
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;

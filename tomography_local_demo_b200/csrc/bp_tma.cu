@@ -222,7 +222,7 @@ __device__ __forceinline__ ViewMeta view_meta(const mr_view& V, const mr_grid& g
 template <int KIND, typename T>
 __global__ void __launch_bounds__(ST_THREADS)
 bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__ ring, int R, int C,
-                 int pitch, long long slot_stride, const mr_view* __restrict__ views,
+                 int pitch, long long slot_stride, int n_slots, const mr_view* __restrict__ views,
                  const mr_grid* __restrict__ grids, const mr_tile* __restrict__ tiles,
                  float* __restrict__ out, int* status, const int64_t* __restrict__ n_tiles_dev,
                  unsigned int* __restrict__ counter, long long tile_cap) {
@@ -288,8 +288,10 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
         __syncthreads();
         const mr_grid& g = s_g;
         // this CTA's share of the views: [v_begin, v_end)
-        const int v_begin = (int)(((long long)g.n_views * crank) / csize);
-        const int v_end = (int)(((long long)g.n_views * (crank + 1)) / csize);
+        int first, count;                   // the grid's slots [first, first + count)
+        grid_view_range(g.view_begin, g.n_views, n_slots, &first, &count);
+        const int v_begin = first + (int)(((long long)count * crank) / csize);
+        const int v_end = first + (int)(((long long)count * (crank + 1)) / csize);
         const int nv = v_end - v_begin;
 
         const float ox = g.origin[0] + t.i0 * g.step_i[0] + t.j0 * g.step_j[0] + t.k * g.step_k[0];
@@ -435,7 +437,8 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                 if (i < g.n_i && j < g.n_j) {
                     const long long o = g.out_offset + (long long)i * g.out_stride_i +
                                         (long long)j * g.out_stride_j + (long long)t.k * g.out_stride_k;
-                    out[o] = inside[p] ? acc[p] * g.scale : 0.f;
+                    const float val = inside[p] ? acc[p] * g.scale : 0.f;
+                    out[o] = g.accumulate ? out[o] + val : val;
                 }
             }
         }
@@ -509,17 +512,17 @@ static int launch_staged(const mr_ring* ring, const mr_view* views, const mr_gri
         MR_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), st));
         cfg.gridDim = dim3((unsigned)(clusters * ST_CLUSTER));
         MR_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, map, static_cast<const T*>(ring->data), ring->rows, ring->cols,
-                                       ring->col_pitch, (long long)ring->slot_stride, views, grids, tiles, out,
-                                       status, n_tiles_dev, counter, (long long)n_tiles));
+                                       ring->col_pitch, (long long)ring->slot_stride, (int)ring->n_slots, views,
+                                       grids, tiles, out, status, n_tiles_dev, counter, (long long)n_tiles));
     } else {
         const int64_t max_chunk = 2147483647LL / ST_CLUSTER;
         for (int64_t t0 = 0; t0 < n_tiles; t0 += max_chunk) {
             const int64_t n = (n_tiles - t0) < max_chunk ? (n_tiles - t0) : max_chunk;
             cfg.gridDim = dim3((unsigned)(n * ST_CLUSTER));
             MR_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, map, static_cast<const T*>(ring->data), ring->rows,
-                                           ring->cols, ring->col_pitch, (long long)ring->slot_stride, views,
-                                           grids, tiles + t0, out, status, (const int64_t*)nullptr,
-                                           (unsigned int*)nullptr, (long long)n));
+                                           ring->cols, ring->col_pitch, (long long)ring->slot_stride,
+                                           (int)ring->n_slots, views, grids, tiles + t0, out, status,
+                                           (const int64_t*)nullptr, (unsigned int*)nullptr, (long long)n));
         }
     }
     MR_CUDA_TRY(cudaGetLastError());

@@ -25,6 +25,15 @@ void set_last_cuda_error(cudaError_t e);
 namespace mr {
 
 // Stored-element loads through the read-only path, widened to FP32.
+// Slots a grid sums: [first, first + count) = [view_begin, view_begin + n_views) clamped
+// to the ring's n_slots, so that a descriptor running past the ring reads nothing outside it.
+__device__ __forceinline__ void grid_view_range(int view_begin, int n_views, int n_slots, int* first,
+                                                int* count) {
+    const int b = min(max(view_begin, 0), max(n_slots, 0));
+    *first = b;
+    *count = max(min(n_views, n_slots - b), 0);
+}
+
 __device__ __forceinline__ float ld_elem(const float* p) { return __ldg(p); }
 __device__ __forceinline__ float ld_elem(const __nv_bfloat16* p) {
     const unsigned short u = __ldg(reinterpret_cast<const unsigned short*>(p));

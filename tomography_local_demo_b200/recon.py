@@ -227,6 +227,8 @@ def _handoff(stream, *tensors):
 
 
 def _struct_tensor(records, device):
+    """Device copy of numpy ABI records (a small pageable copy on the current stream: it is
+    not queued behind large pinned transfers that other streams have in flight)."""
     raw = np.ascontiguousarray(records).view(np.uint8)
     return torch.from_numpy(raw.copy()).to(device, non_blocking=False)
 
@@ -553,6 +555,9 @@ class SliceReconstructor:
             with torch.cuda.device(self.device):
                 self._proj = torch.zeros((self.n_total, R, self._pitch), dtype=torch.float32, device=self.device)
         self._ingest_event = None
+        # (slot_end, event) of the chunks of the latest host upload: a reconstruction can
+        # sum the views of each chunk as soon as that chunk is filtered
+        self._chunk_marks = []
         self._raw_dev = None            # device staging of host raw counts (grows on demand)
         self._raw_pinned = []           # pinned staging of pageable raw counts, one per chunk slot
         self.upload_chunk_bytes = 16 << 20   # raw bytes per overlapped upload + ingest chunk
@@ -579,20 +584,27 @@ class SliceReconstructor:
         K = {k: v[idx] for k, v in self._K_all.items()}
         return cone_filter_views(K, R, C, n_fft, slots)
 
-    def _admit(self, indices, slots, event):
+    def _upload_view_records(self, indices, slots):
+        """Queue the mr_view records of new slots on the ingest stream (asynchronous)."""
+        n0, n1 = slots[0], slots[-1] + 1
+        recs = np.ascontiguousarray(self._maps_all[indices]).view(np.uint8)
+        with torch.cuda.stream(self.ingest_stream):
+            dst = self._views_dev[n0 * N.VIEW_DTYPE.itemsize:n1 * N.VIEW_DTYPE.itemsize]
+            # pinned source: the copy is asynchronous and the host does not wait for the
+            # ingest kernels queued before it (the caching host allocator keeps the
+            # buffer alive until the copy has run)
+            dst.copy_(torch.from_numpy(recs.copy()).pin_memory(), non_blocking=True)
+
+    def _admit(self, indices, slots, event, uploaded=False, marks=()):
         """Make filtered slots visible to reconstructions (under the state lock)."""
         with self._lock:
             n0, n1 = slots[0], slots[-1] + 1
             self._order[n0:n1] = indices
             self._received[indices] = True
             self._views_host[n0:n1] = self._maps_all[indices]
-            rec = self._views_host[n0:n1].view(np.uint8)
-            with torch.cuda.stream(self.ingest_stream):
-                dst = self._views_dev[n0 * N.VIEW_DTYPE.itemsize:n1 * N.VIEW_DTYPE.itemsize]
-                # pinned source: the copy is asynchronous and the host does not wait for the
-                # ingest kernels queued before it (the caching host allocator keeps the
-                # buffer alive until the copy has run)
-                dst.copy_(torch.from_numpy(rec.copy()).pin_memory(), non_blocking=True)
+            if not uploaded:
+                self._upload_view_records(indices, slots)
+            self._chunk_marks = list(marks)
             event.record(self.ingest_stream)
             self._ingest_event = event
             self.n = n1
@@ -639,6 +651,7 @@ class SliceReconstructor:
             ev.record(self.stream)
             self.ingest_stream.wait_event(ev)
             self._received[:] = False
+            self._chunk_marks = []
             self.n = 0
             self.version += 1
 
@@ -702,24 +715,34 @@ class SliceReconstructor:
             k = len(indices)
             n0 = self.n
             slots = np.arange(n0, n0 + k)
-            fv_host = self._filter_views(indices, slots)
             on_device = isinstance(raw, torch.Tensor) and raw.is_cuda
             if self._proj is not None:
                 self._keep_raw_line_integrals(raw, n0, k)
-            with torch.cuda.device(self.device), torch.cuda.stream(self.ingest_stream):
+
+            def prepare():
+                # filter records of the new slots and their view records, queued on the
+                # ingest stream ahead of the first ingest launch (the view records go
+                # before any chunk is filtered, so a reconstruction may use the first
+                # chunks of this call while the later ones are still on the bus)
+                fv_host = self._filter_views(indices, slots)
                 fv_pinned = torch.from_numpy(np.ascontiguousarray(fv_host).view(np.uint8).copy()).pin_memory()
                 fv = fv_pinned.to(self.device, non_blocking=True)
+                self._upload_view_records(indices, slots)
+                return fv
+
+            marks = []
+            with torch.cuda.device(self.device), torch.cuda.stream(self.ingest_stream):
                 if on_device:
                     x = raw.view(torch.int16) if raw.dtype == torch.uint16 else raw
                     x = x.to(self.device, non_blocking=True).contiguous()
                     if x.element_size() != 2:
                         raise ValueError("raw counts must be 16-bit")
-                    self._ingest_launch(x, 0, k, fv)
+                    self._ingest_launch(x, 0, k, prepare())
                     x.record_stream(self.ingest_stream)
                 else:
-                    self._ingest_host(raw, k, fv)
+                    marks = [(n0 + c1, e) for c1, e in self._ingest_host(raw, k, prepare)[:-1]]
                 ev = torch.cuda.Event()
-            return self._admit(indices, slots, ev)
+            return self._admit(indices, slots, ev, uploaded=True, marks=marks)
 
     def _keep_raw_line_integrals(self, raw, n0, k):
         """-log(max((binned counts - dark) * gain, 1e-3)) of k raw views into the kept
@@ -824,11 +847,14 @@ class SliceReconstructor:
             tm.stop(name, ev0, self.ingest_stream)
         N.check(st, name)
 
-    def _ingest_host(self, raw, k, fv):
+    def _ingest_host(self, raw, k, prepare):
         """Upload host raw counts in chunks on the copy stream and filter each chunk on the
         ingest stream as soon as it has landed, so the PCIe transfer of chunk i+1 overlaps
         the ingest of chunk i. Pinned torch tensors are copied directly; anything else
-        (NumPy, pageable tensors) is staged through reusable pinned buffers."""
+        (NumPy, pageable tensors) is staged through reusable pinned buffers. `prepare()`
+        (host-side records of the new views, returning the device filter records) runs
+        once the first chunk is on the bus, so the transfer does not wait for it.
+        Returns [(views done, event)] per chunk."""
         if isinstance(raw, torch.Tensor):
             if raw.element_size() != 2:
                 raise ValueError("raw counts must be 16-bit")
@@ -851,6 +877,7 @@ class SliceReconstructor:
         x = self._raw_dev[:need].view(k, shape[1], shape[2])
         # the previous call's ingest kernels must be done reading the staging buffer
         self.copy_stream.wait_stream(self.ingest_stream)
+        marks = []                      # (views done, event) per chunk
         if not pinned:
             n_slots = 3
             while len(self._raw_pinned) < n_slots:
@@ -874,8 +901,14 @@ class SliceReconstructor:
                     slot[1].record(self.copy_stream)
                 landed = torch.cuda.Event()
                 landed.record(self.copy_stream)
+            if i == 0:
+                fv = prepare()
             self.ingest_stream.wait_event(landed)
             self._ingest_launch(x, c0, c1, fv)
+            done = torch.cuda.Event()
+            done.record(self.ingest_stream)
+            marks.append((c1, done))
+        return marks
 
     # ----------------------------------------------------------- info
     @property
@@ -904,12 +937,51 @@ class SliceReconstructor:
             return self.n, self.cor_shift, self._ingest_event
 
     def _run_grids(self, grids, out, n, event):
-        """Launch one batched back-projection of `grids` into device `out`."""
+        """Launch the batched back-projection of `grids` into device `out`. Right after a
+        chunked host upload, the views are summed chunk by chunk: each partial launch
+        waits only for its own chunk's filter, so the reconstruction overlaps the transfer
+        of the later chunks (same scale; FP32 partial sums added in view order)."""
         stream = self.stream
+        grids["scale"] = np.pi / n if n else 0.0
+        marks = [(se, e) for se, e in self._chunk_marks if 0 < se < n]
+        regular = not (np.asarray(grids["flags"]) & N.MR_GRID_POINTS).any()
+        if marks and regular and self.bp_kernel == "staged":
+            bounds = [0] + [se for se, _ in marks] + [n]
+            events = [e for _, e in marks] + [event]
+            G = len(grids)
+            parts = np.tile(np.ascontiguousarray(grids, dtype=N.GRID_DTYPE), len(events))
+            for i, (a, b) in enumerate(zip(bounds[:-1], bounds[1:])):
+                sl = slice(i * G, (i + 1) * G)
+                parts["view_begin"][sl], parts["n_views"][sl] = a, b - a
+                parts["accumulate"][sl] = 0 if i == 0 else 1
+            tiles = N.plan_tiles(grids)              # the same tiles for every view range
+            if len(tiles) == 0:
+                return
+            lib = N.load()
+            v = ctypes_void
+            with torch.cuda.device(self.device), torch.cuda.stream(stream):
+                # one upload for all ranges; launch i reads its own G records
+                g_dev = _struct_tensor(parts, self.device)
+                t_dev = _struct_tensor(tiles, self.device)
+                st_ptr = v(self._status.data_ptr())
+                for i, ((a, b), e) in enumerate(zip(zip(bounds[:-1], bounds[1:]), events)):
+                    if e is not None:
+                        stream.wait_event(e)
+                    tm = self.kernel_timer
+                    ev0 = tm.start(stream) if tm is not None else None
+                    rc = lib.mr_backproject_staged(self._ring_c, v(self._views_dev.data_ptr()),
+                                                   v(g_dev.data_ptr() + i * G * N.GRID_DTYPE.itemsize),
+                                                   v(t_dev.data_ptr()), len(tiles), v(out.data_ptr()), st_ptr,
+                                                   v(stream.cuda_stream))
+                    if tm is not None:
+                        tm.stop("mr_backproject_staged", ev0, stream)
+                    N.check(rc, "mr_backproject_staged")
+                g_dev.record_stream(stream)
+                t_dev.record_stream(stream)
+            return
         if event is not None:
             stream.wait_event(event)
         grids["n_views"] = n
-        grids["scale"] = np.pi / n if n else 0.0
         with torch.cuda.device(self.device), torch.cuda.stream(stream):
             backproject_device(self._ring_c, self._views_dev, grids, out, stream, self.device,
                                self.kernel_timer, self.bp_kernel, self._status)
@@ -979,9 +1051,16 @@ class SliceReconstructor:
 
     def reconstruct_planes(self, requests):
         """Batched reconstruct_plane without the point arrays: list of f64 images
-        (one device->host copy for the whole batch)."""
+        (one device->host copy for the whole batch). The images are widened to f64 on the
+        device and copied into one pinned host buffer, which the returned arrays view
+        (the pinned block goes back to torch's host cache when they are freed)."""
         out, sizes = self._planes(requests)
-        host = out.cpu().numpy().astype(np.float64)
+        pinned = torch.empty(out.shape, dtype=torch.float64, pin_memory=True)
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            wide = out.to(torch.float64)
+            pinned.copy_(wide, non_blocking=True)
+        self.stream.synchronize()
+        host = pinned.numpy()
         res, o = [], 0
         for n in sizes:
             res.append(host[o:o + n * n].reshape(n, n))
