@@ -297,6 +297,34 @@ int mr_ingest_u16_tc(const uint16_t* raw, int64_t s_view, int64_t s_row,
 int mr_slice_entropy(const float* imgs, int32_t n_imgs, int64_t stride, int32_t n_pix,
                      int32_t bins, double* scores_dev, void* stream);
 
+/* ---- volume consumers -----------------------------------------------------------
+ * The device passes of model.py:18-29 (otsu_threshold) over a reconstructed volume of
+ * n f32 voxels (device, 4-byte aligned, any layout): the host computes the percentile
+ * interpolation and the Otsu sums over the bins in FP64 from what these return.
+ * ws: device workspace of mr_volume_workspace_bytes() bytes (8-byte aligned), shared by
+ * the three calls of one threshold; calls on one workspace must not overlap. */
+int64_t mr_volume_workspace_bytes(void);
+
+/* Counts of the voxels != 0 and of the NaN voxels, and the order keys of the smallest
+ * and largest non-zero, non-NaN value (key = bits | 2^31 for x >= 0, ~bits for x < 0).
+ * stats_host (optional, host): {nonzero, nan, kmin | (uint64_t)kmax << 32}; when given,
+ * the call waits for the stream. */
+int mr_volume_stats(const float* vol, int64_t n, void* ws, uint64_t* stats_host, void* stream);
+
+/* The values of rank ranks[j] (0-based, ascending) among the non-zero, non-NaN voxels,
+ * j < n_ranks <= 4, into values_dev (device, n_ranks floats): exact order statistics
+ * (a radix select over the bits in which kmin and kmax, from mr_volume_stats, differ). */
+int mr_volume_select(const float* vol, int64_t n, const int64_t* ranks_host, int32_t n_ranks,
+                     uint32_t kmin, uint32_t kmax, void* ws, float* values_dev, void* stream);
+
+/* hist_dev[b] (device, bins uint64, overwritten) = the number of non-zero, non-NaN voxels
+ * whose FP64 value clipped to [lo, hi] falls in bin b of numpy.histogram(..., bins,
+ * range=(lo, hi)): edges_dev (device, bins + 1 doubles) = np.linspace(first, last,
+ * bins + 1) with (first, last) = (lo, hi), widened by 0.5 on each side if lo == hi; a value
+ * on an inner edge counts in the bin above it, the top edge in the last bin. bins <= 2048. */
+int mr_volume_histogram(const float* vol, int64_t n, const double* edges_dev, int32_t bins,
+                        double lo, double hi, uint64_t* hist_dev, void* stream);
+
 /* ---- pre-processing on arrival (block layout [rows, k, cols], f32, device) ------
  * Replaces preprocess.py:31-56 (rotate_projections): every projection rotated by
  * `degrees` about the detector centre, bilinear, zero outside. in != out. */

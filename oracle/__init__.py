@@ -11,6 +11,7 @@ function by function - each function cites the reference file:line it follows:
   phantom.py  phantom.py analytic ellipsoid projector (fixture generator)
   recon.py    SliceReconstructor pipeline (recon.py:289-519) at FP32-store / FP64
   ls.py       few-view least-squares slice refinement (no reference counterpart)
+  model.py    otsu_threshold of the volume consumer (model.py:18-29)
 Parity of this restatement is pinned against golden vectors produced by the reference
 itself (tests/golden/make_golden.py, fixtures in tests/golden/*.npz).
 """

@@ -75,6 +75,10 @@ SIGNATURES = {
     "mr_ingest_u16_tc": (ctypes.c_int, [_P, _I64, _I64, _I32, _I32, _P, _P, _I32, _P, _P, _I32, ctypes.c_float,
                                         _I32, ctypes.POINTER(MrRing), _P, _P]),
     "mr_slice_entropy": (ctypes.c_int, [_P, _I32, _I64, _I32, _I32, _P, _P]),
+    "mr_volume_workspace_bytes": (_I64, []),
+    "mr_volume_stats": (ctypes.c_int, [_P, _I64, _P, _P, _P]),
+    "mr_volume_select": (ctypes.c_int, [_P, _I64, _P, _I32, ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P]),
+    "mr_volume_histogram": (ctypes.c_int, [_P, _I64, _P, _I32, ctypes.c_double, ctypes.c_double, _P, _P]),
     "mr_rotate_f32": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, ctypes.c_double, _P]),
     "mr_gaussian_axis_f32": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _I32, _I32, _P, _I32, _P]),
 }

@@ -14,10 +14,11 @@ constexpr int ENT_THREADS = 512;
 constexpr int ENT_MAX_BINS = 1024;
 
 __device__ __forceinline__ double edge(double lo, double hi, int b, int bins) {
-    // np.linspace(lo, hi, bins + 1): lo + b * step (the last edge exactly hi)
+    // np.linspace(lo, hi, bins + 1): (b * step) + lo, each step rounded on its own (no FMA
+    // contraction), the last edge exactly hi
     if (b >= bins) return hi;
-    const double step = (hi - lo) / bins;
-    return lo + b * step;
+    const double step = __ddiv_rn(__dsub_rn(hi, lo), (double)bins);
+    return __dadd_rn(__dmul_rn((double)b, step), lo);
 }
 
 __global__ void __launch_bounds__(ENT_THREADS)
@@ -60,7 +61,7 @@ entropy_kernel(const float* __restrict__ imgs, long long stride, int n_pix, int 
         const float vf = img[i];
         if (vf == 0.f) continue;
         const double v = vf;
-        int k = (int)(((v - lo) / denom) * bins);      // numpy: ((x - lo) / (hi - lo)) * bins
+        int k = (int)__dmul_rn(__ddiv_rn(__dsub_rn(v, lo), denom), (double)bins);   // ((x - lo) / (hi - lo)) * bins
         if (k >= bins) k = bins - 1;
         if (k < 0) k = 0;
         if (v < edge(lo, hi, k, bins)) --k;
