@@ -4,8 +4,8 @@
 // reduced to three streaming passes over the volume (any number of voxels, FP32):
 //   mr_volume_stats      count of non-zero voxels and NaNs, min / max order key
 //   mr_volume_select     exact order statistics of the non-zero voxels (radix select on
-//                        order-preserving keys, 8-bit digits below the bits that the
-//                        smallest and largest key share: at most 4 passes)
+//                        order-preserving keys, 11-bit digits below the bits that the
+//                        smallest and largest key share: at most 3 passes)
 //   mr_volume_histogram  numpy's uniform-bin histogram of the FP64-clipped values
 // The percentile interpolation and the Otsu arithmetic over the bins stay on the host,
 // in FP64 as the reference computes them.
@@ -21,6 +21,8 @@ namespace mr {
 constexpr int VOL_THREADS = 256;
 constexpr int VOL_MAX_RANKS = 4;
 constexpr int VOL_MAX_BINS = 2048;
+constexpr int VOL_RADIX = 11;                   // digit bits of one select pass
+constexpr int VOL_DIGITS = 1 << VOL_RADIX;
 constexpr uint32_t VOL_NONE = 0xffffffffu;
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -31,7 +33,7 @@ struct VolState {
     unsigned int kmin, kmax;                // order keys of the smallest / largest non-NaN value != 0
     unsigned int prefix[VOL_MAX_RANKS];     // key bits found so far, per requested rank
     unsigned long long rank[VOL_MAX_RANKS]; // rank left inside the current prefix
-    unsigned long long hist[VOL_MAX_RANKS][256];
+    unsigned long long hist[VOL_MAX_RANKS][VOL_DIGITS];
 };
 
 // Order-preserving map of a float onto an unsigned key (negatives reversed below positives).
@@ -127,13 +129,14 @@ vol_stats_kernel(const float* __restrict__ v, long long n, VolState* st) {
 
 // One radix digit for every requested rank: voxels whose key matches the rank's prefix
 // above the digit count into that rank's 2^width bins. shared = 1: all ranks still share
-// their prefix, so one histogram serves them all.
+// their prefix, so one histogram serves them all. After the first pass a prefix covers a
+// small part of the voxels, so a warp whose voxels match no prefix moves on after one vote.
 __global__ void __launch_bounds__(VOL_THREADS)
 vol_select_pass_kernel(const float* __restrict__ v, long long n, VolState* st, int n_ranks, int shared,
                        int shift, int width, uint32_t mask_hi) {
-    __shared__ unsigned int h[VOL_MAX_RANKS][256];
+    __shared__ unsigned int h[VOL_MAX_RANKS][VOL_DIGITS];
     const int n_hist = shared ? 1 : n_ranks;
-    for (int i = threadIdx.x; i < VOL_MAX_RANKS * 256; i += blockDim.x) (&h[0][0])[i] = 0u;
+    for (int i = threadIdx.x; i < n_hist * VOL_DIGITS; i += blockDim.x) (&h[0][0])[i] = 0u;
     uint32_t pre[VOL_MAX_RANKS];
 #pragma unroll
     for (int j = 0; j < VOL_MAX_RANKS; ++j) pre[j] = st->prefix[j] & mask_hi;
@@ -143,27 +146,40 @@ vol_select_pass_kernel(const float* __restrict__ v, long long n, VolState* st, i
     for_each_voxel(v, n, [&](float x, bool ok) {
         const bool live = ok && x != 0.f && x == x;
         const uint32_t k = order_key(x);
+        const uint32_t hi = k & mask_hi;
+        bool m[VOL_MAX_RANKS];
+        bool any = false;
+#pragma unroll
+        for (int j = 0; j < VOL_MAX_RANKS; ++j) {
+            m[j] = live && j < n_hist && hi == pre[j];
+            any |= m[j];
+        }
+        if (!__any_sync(FULL, any)) return;                 // warp-uniform
         const uint32_t d = (k >> shift) & dmask;
 #pragma unroll
         for (int j = 0; j < VOL_MAX_RANKS; ++j) {
-            if (j < n_hist)                                 // block-uniform
-                warp_run_add(h[j], live && (k & mask_hi) == pre[j] ? d : VOL_NONE, lane);
+            if (j < n_hist && __any_sync(FULL, m[j]))       // warp-uniform
+                warp_run_add(h[j], m[j] ? d : VOL_NONE, lane);
         }
     });
     __syncthreads();
-    for (int i = threadIdx.x; i < n_hist * 256; i += blockDim.x) {
+    for (int i = threadIdx.x; i < n_hist * VOL_DIGITS; i += blockDim.x) {
         const unsigned int c = (&h[0][0])[i];
-        if (c) atomicAdd(&st->hist[i >> 8][i & 255], (unsigned long long)c);
+        if (c) atomicAdd(&st->hist[i / VOL_DIGITS][i % VOL_DIGITS], (unsigned long long)c);
     }
 }
 
 // Picks each rank's digit from its histogram (exclusive prefix sums over the bins), narrows
-// the rank, clears the histograms. One block of 256 threads.
+// the rank, clears the histograms. One block of 256 threads, 8 bins per thread.
 __global__ void __launch_bounds__(256) vol_select_pick_kernel(VolState* st, int n_ranks, int shared, int shift) {
+    constexpr int PER = VOL_DIGITS / 256;
     __shared__ unsigned long long warp_tot[8];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     for (int j = 0; j < n_ranks; ++j) {
-        const unsigned long long c = st->hist[shared ? 0 : j][t];
+        const unsigned long long* hj = st->hist[shared ? 0 : j] + t * PER;
+        unsigned long long c = 0;
+#pragma unroll
+        for (int i = 0; i < PER; ++i) c += hj[i];
         unsigned long long incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -175,16 +191,18 @@ __global__ void __launch_bounds__(256) vol_select_pick_kernel(VolState* st, int 
         unsigned long long off = 0;
         for (int w = 0; w < warp; ++w) off += warp_tot[w];
         incl += off;
-        const unsigned long long excl = incl - c;
+        unsigned long long excl = incl - c;
         const unsigned long long r = st->rank[j];
         __syncthreads();                    // every thread has read rank[j] and warp_tot
         if (c > 0 && excl <= r && r < incl) {
-            st->prefix[j] |= (uint32_t)t << shift;
+            int b = 0;
+            for (; b < PER - 1 && excl + hj[b] <= r; ++b) excl += hj[b];
+            st->prefix[j] |= (uint32_t)(t * PER + b) << shift;
             st->rank[j] = r - excl;
         }
         __syncthreads();
     }
-    for (int j = 0; j < VOL_MAX_RANKS; ++j) st->hist[j][t] = 0ull;
+    for (int i = t; i < VOL_MAX_RANKS * VOL_DIGITS; i += 256) (&st->hist[0][0])[i] = 0ull;
 }
 
 struct RankList {
@@ -197,7 +215,7 @@ __global__ void vol_select_init_kernel(VolState* st, RankList ranks, int n_ranks
         st->prefix[j] = prefix;
         st->rank[j] = j < n_ranks ? (unsigned long long)ranks.r[j] : 0ull;
     }
-    for (int i = threadIdx.x; i < VOL_MAX_RANKS * 256; i += blockDim.x) (&st->hist[0][0])[i] = 0ull;
+    for (int i = threadIdx.x; i < VOL_MAX_RANKS * VOL_DIGITS; i += blockDim.x) (&st->hist[0][0])[i] = 0ull;
 }
 
 __global__ void vol_select_out_kernel(const VolState* st, int n_ranks, float* out) {
@@ -205,29 +223,48 @@ __global__ void vol_select_out_kernel(const VolState* st, int n_ranks, float* ou
     if (j < n_ranks) out[j] = key_value(st->prefix[j]);
 }
 
-// np.histogram(np.clip(v, lo, hi), bins, range) over the non-zero voxels: the bin from the
-// FP64 clipped value scaled to the range, then moved to the bin whose edges (numpy's FP64
-// linspace, passed in) enclose the value - the top edge counted in the last bin. numpy's
-// own rule (index from ((x - first) / (last - first)) * bins, corrected by one step
-// against the same edges) gives the same bin whenever its first estimate is within one
-// bin, i.e. always for finite ranges.
+// np.histogram(np.clip(v, lo, hi), bins, range) over the non-zero voxels, in FP32: a float
+// x lies in bin k (edges[k] <= x < edges[k+1], FP64 edges = numpy's linspace, passed in)
+// exactly when lb[k] <= x < lb[k+1], lb[i] = edges[i] rounded up to a float (the smallest
+// float >= the edge); the top edge counts in the last bin. The clip is exact the same way:
+// x < lo exactly when x < lo rounded up, x > hi exactly when x > hi rounded down, and those
+// voxels take the bin of lo / hi. numpy's own rule (index from ((x - first) / (last -
+// first)) * bins, corrected by one step against the same edges) lands in the same bin.
 __global__ void __launch_bounds__(VOL_THREADS)
 vol_histogram_kernel(const float* __restrict__ v, long long n, const double* __restrict__ edges, int bins,
-                     double lo, double hi, double first, double scale, unsigned long long* __restrict__ hist) {
+                     double lo, double hi, unsigned long long* __restrict__ hist) {
     __shared__ unsigned int h[VOL_MAX_BINS];
-    __shared__ double e[VOL_MAX_BINS + 1];
+    __shared__ float lb[VOL_MAX_BINS + 1];
+    __shared__ int s_bin_lo, s_bin_hi;
     for (int i = threadIdx.x; i < bins; i += blockDim.x) h[i] = 0u;
-    for (int i = threadIdx.x; i <= bins; i += blockDim.x) e[i] = edges[i];
+    for (int i = threadIdx.x; i <= bins; i += blockDim.x) lb[i] = __double2float_ru(edges[i]);
+    if (threadIdx.x == 0) {
+        // bins of the clip bounds themselves (lo, hi inside [edges[0], edges[bins]])
+        int a = 0, b = bins - 1;
+        while (a < bins - 1 && lo >= edges[a + 1]) ++a;
+        while (b > 0 && hi < edges[b]) --b;
+        s_bin_lo = a;
+        s_bin_hi = b;
+    }
     __syncthreads();
+    const float lo_up = __double2float_ru(lo), hi_dn = __double2float_rd(hi);
+    const float first = lb[0], scale = (float)bins / (lb[bins] - lb[0]);
+    const int bin_lo = s_bin_lo, bin_hi = s_bin_hi;
     const int lane = threadIdx.x & 31;
     for_each_voxel(v, n, [&](float x, bool ok) {
         uint32_t b = VOL_NONE;
         if (ok && x != 0.f && x == x) {
-            const double xd = fmin(fmax((double)x, lo), hi);
-            const double f = __dmul_rn(__dsub_rn(xd, first), scale);
-            int k = f >= (double)bins ? bins - 1 : (f > 0.0 ? (int)f : 0);
-            while (k > 0 && xd < e[k]) --k;
-            while (k < bins - 1 && xd >= e[k + 1]) ++k;
+            int k;
+            if (x < lo_up) {
+                k = bin_lo;
+            } else if (x > hi_dn) {
+                k = bin_hi;
+            } else {
+                const float f = (x - first) * scale;
+                k = f >= (float)bins ? bins - 1 : (f > 0.f ? (int)f : 0);
+                while (k > 0 && x < lb[k]) --k;
+                while (k < bins - 1 && x >= lb[k + 1]) ++k;
+            }
             b = (uint32_t)k;
         }
         warp_run_add(h, b, lane);
@@ -288,8 +325,8 @@ extern "C" int mr_volume_select(const float* vol, int64_t n, const int64_t* rank
     const int L = (kmin == kmax) ? 0 : 32 - __builtin_clz(kmin ^ kmax);
     const uint32_t known = L >= 32 ? 0u : ~((1u << L) - 1u);
     mr::vol_select_init_kernel<<<1, 256, 0, st>>>(s, rl, n_ranks, kmin & known);
-    for (int top = L, pass = 0; top > 0; top -= 8, ++pass) {
-        const int shift = top > 8 ? top - 8 : 0;
+    for (int top = L, pass = 0; top > 0; top -= mr::VOL_RADIX, ++pass) {
+        const int shift = top > mr::VOL_RADIX ? top - mr::VOL_RADIX : 0;
         const int width = top - shift;
         const uint32_t mask_hi = top >= 32 ? 0u : ~((1u << top) - 1u);
         const int shared = pass == 0 ? 1 : 0;
@@ -319,8 +356,7 @@ extern "C" int mr_volume_histogram(const float* vol, int64_t n, const double* ed
     if (rc != MR_OK) return rc;
     if (n > 0)
         mr::vol_histogram_kernel<<<blocks, mr::VOL_THREADS, 0, st>>>(
-            vol, (long long)n, edges_dev, bins, lo, hi, first, scale,
-            reinterpret_cast<unsigned long long*>(hist_dev));
+            vol, (long long)n, edges_dev, bins, lo, hi, reinterpret_cast<unsigned long long*>(hist_dev));
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;
 }
