@@ -254,6 +254,25 @@ int mr_ingest_u16(const uint16_t* raw, int64_t s_view, int64_t s_row,
                   const float* H_dev, const float* twiddle_dev, int32_t log2n,
                   const mr_ring* ring, void* stream);
 
+/* ---- raw correction alone (the scan loaders' output stack) ------------------------
+ * Replaces the per-projection correction of flexray.py:111-116 + 174-184 (`corrected`,
+ * mode MR_CORRECT_FLEXRAY: float32 bin mean, (mean - dark) * scale, scale = the gain
+ * 1/max(F-D, 1)) and of hdf5.py:24-31 + 73-78 (mode MR_CORRECT_HDF5: float64 bin mean
+ * rounded to float32, (mean - dark) / scale, scale = max(F-D, 1e-6)), then clip 1e-3 and
+ * -log, with the loaders' detector crop:
+ *   out[r*so_row + v*so_view + c] = -log(max(t, 1e-3)) for v < k, r < rows, c < cols,
+ * t from the bin x bin mean of raw (uint16, device, view v at raw + v*s_view, row stride
+ * s_row) at full binned row y = row0 + r (raw row flip ? rows_full-1-y : y, i.e. the frame
+ * flipped upside down before the crop) and binned column x = col0 + c, and from
+ * dark[y*s_frame + x], scale[y*s_frame + x] (device f32, the full binned frame in output
+ * orientation). bin <= 16; k, rows <= 65535. */
+#define MR_CORRECT_FLEXRAY 0
+#define MR_CORRECT_HDF5    1
+int mr_correct_u16(const uint16_t* raw, int64_t s_view, int64_t s_row, int32_t k, int32_t bin,
+                   int32_t flip_rows, int32_t rows_full, int32_t row0, int32_t col0, int32_t rows,
+                   int32_t cols, const float* dark_dev, const float* scale_dev, int64_t s_frame,
+                   int32_t mode, float* out_dev, int64_t so_row, int64_t so_view, void* stream);
+
 /* ---- tensor-core Toeplitz filter (the measured alternative to the FFT filter) ------
  * Same contracts as mr_filter_f32 / mr_ingest_u16 (recon.py:58-104; flexray.py:174-184 +
  * hdf5.py:73-78 for the raw correction), with the row filter computed as a GEMM on the

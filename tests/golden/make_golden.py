@@ -173,7 +173,29 @@ def main(ref_root):
     vol = rng.gamma(2.0, 0.1, (10, 11, 12)).astype(np.float32)
     vol[vol < 0.05] = 0
     save("misc.npz", otsu_vol=vol, otsu=M.otsu_threshold(vol), **d)
+    loader_fixtures(FX, H5, save)
     print("golden fixtures written to", HERE, "from minirecast", minirecast.__version__)
+
+
+def loader_fixtures(FX, H5, save):
+    """The reference loaders with the detector crop, the object box, skip, and an HDF5 scan
+    without flat / dark frames, on the deterministic scans of scan_synth.py."""
+    sys.path.insert(0, HERE)
+    import scan_synth as SS
+    tmp = tempfile.mkdtemp(prefix="flexray_crop_")
+    SS.write_flexray_scan(tmp)
+    out = {}
+    for tag, kw in (("s2", dict(sample=2, skip=1)), ("s2k2", dict(sample=2, skip=2)),
+                    ("s3", dict(sample=3, skip=1, profile="cwi-flexray-2022-10-28"))):
+        kw.setdefault("profile", "cwi-flexray-2019-04-24")
+        proj, geom = FX.load_flexray(tmp, crop=True, auto_box=True, verbose=False, **kw)
+        out[f"{tag}_proj"], out[f"{tag}_V"], out[f"{tag}_box"] = proj, geom.vectors, geom.box
+    out["settings"] = np.array(FX.parse_scan_settings(tmp)["det_tan"])
+    for tag, kw in (("nf", dict(sample=2, skip=2, rows="2:30")), ("wf", dict(sample=1, skip=1))):
+        files = SS.dxchange_arrays(flat=(tag == "wf"))
+        proj, geom = H5.load_dxchange("fake.h5", h5=SS.FakeH5(files), verbose=False, **kw)
+        out[f"h5{tag}_proj"], out[f"h5{tag}_angles"] = proj, geom.angles
+    save("loaders_device.npz", **out)
 
 
 if __name__ == "__main__":

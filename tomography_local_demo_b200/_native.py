@@ -20,6 +20,7 @@ MR_ERR_SCRATCH_LIMIT = -5
 MR_NOALLOC_MAX_TILES = 1 << 31
 
 MR_F32, MR_BF16, MR_F16, MR_U16 = 0, 1, 2, 3
+MR_CORRECT_FLEXRAY, MR_CORRECT_HDF5 = 0, 1
 MR_PARALLEL, MR_CONE = 0, 1
 MR_GRID_MASK_BOX, MR_GRID_POINTS = 1, 2
 
@@ -75,6 +76,8 @@ SIGNATURES = {
     "mr_ingest_u16_tc": (ctypes.c_int, [_P, _I64, _I64, _I32, _I32, _P, _P, _I32, _P, _P, _I32, ctypes.c_float,
                                         _I32, ctypes.POINTER(MrRing), _P, _P]),
     "mr_slice_entropy": (ctypes.c_int, [_P, _I32, _I64, _I32, _I32, _P, _P]),
+    "mr_correct_u16": (ctypes.c_int, [_P, _I64, _I64, _I32, _I32, _I32, _I32, _I32, _I32, _I32, _I32, _P, _P,
+                                       _I64, _I32, _P, _I64, _I64, _P]),
     "mr_volume_workspace_bytes": (_I64, []),
     "mr_volume_stats": (ctypes.c_int, [_P, _I64, _P, _P, _P]),
     "mr_volume_select": (ctypes.c_int, [_P, _I64, _P, _I32, ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P]),

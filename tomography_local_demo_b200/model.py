@@ -20,14 +20,12 @@ from .recon import ctypes_void
 PERCENTILES = (0.1, 99.95)          # the clip range of the reference (model.py:21)
 
 
-def percentile_linear(n, q, order_stat):
-    """numpy.percentile(v, q) (method "linear", numpy 2.x) of n float32 values v, from
-    order_stat(ranks) -> float32 values of those 0-based ascending ranks of v.
-
-    The steps of numpy's own computation: q / float32(100) in FP64, virtual index
-    (n - 1) * q, neighbours floor(index) and floor(index) + 1 (the last value when the
-    index reaches n - 1), their difference in FP32, then a + diff * g in FP64 (or
-    b - diff * (1 - g) for g >= 0.5), g = index - floor(index)."""
+def linear_neighbours(n, q):
+    """numpy's "linear" percentile set-up for n sorted values (numpy 2.x): q / float32(100)
+    in FP64, virtual index (n - 1) * q, neighbours floor(index) and floor(index) + 1 (the
+    last value, rank n - 1, once the index reaches n - 1) and the blend weight
+    g = index - floor(index) (numpy's own g, computed against -1 for the last value).
+    Returns (prev ranks, next ranks, g), arrays over q."""
     if n < 1:
         raise IndexError("index -1 is out of bounds for axis 0 with size 0")
     q = np.true_divide(np.asarray(q, dtype=np.float64), np.float32(100))
@@ -40,16 +38,29 @@ def percentile_linear(n, q, order_stat):
     prev = prev.astype(np.intp)
     nxt = nxt.astype(np.intp)
     gamma = np.asarray(vi - prev, dtype=np.float64)
-    ranks = np.unique(np.concatenate([np.where(prev < 0, n - 1, prev), np.where(nxt < 0, n - 1, nxt)]))
+    return np.where(prev < 0, n - 1, prev), np.where(nxt < 0, n - 1, nxt), gamma
+
+
+def lerp_like_numpy(a, b, gamma):
+    """numpy's percentile blend of float32 neighbours a, b (broadcasting over gamma):
+    their difference in FP32, then a + diff * g in FP64, or b - diff * (1 - g) for g >= 0.5."""
+    a = np.asarray(a, dtype=np.float32)
+    b = np.asarray(b, dtype=np.float32)
+    gamma = np.asarray(gamma, dtype=np.float64)
+    diff = np.subtract(b, a)                        # FP32
+    return np.where(gamma >= 0.5, b - diff * (1 - gamma), a + diff * gamma)     # FP64
+
+
+def percentile_linear(n, q, order_stat):
+    """numpy.percentile(v, q) (method "linear", numpy 2.x) of n float32 values v, from
+    order_stat(ranks) -> float32 values of those 0-based ascending ranks of v."""
+    prev, nxt, gamma = linear_neighbours(n, q)
+    ranks = np.unique(np.concatenate([prev, nxt]))
     vals = np.asarray(order_stat(ranks), dtype=np.float32)
     lookup = dict(zip(ranks.tolist(), vals))
-    a = np.array([lookup[int(n - 1 if i < 0 else i)] for i in prev], dtype=np.float32)
-    b = np.array([lookup[int(n - 1 if i < 0 else i)] for i in nxt], dtype=np.float32)
-    diff = np.subtract(b, a)                        # FP32, as numpy's _lerp
-    out = np.add(a, diff * gamma)                   # FP64
-    upper = gamma >= 0.5
-    out[upper] = (b - diff * (1 - gamma))[upper]
-    return out
+    a = np.array([lookup[int(i)] for i in prev], dtype=np.float32)
+    b = np.array([lookup[int(i)] for i in nxt], dtype=np.float32)
+    return lerp_like_numpy(a, b, gamma)
 
 
 def _device_volume(vol):
