@@ -325,7 +325,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // PREF: the next item's two input rows are copied to shared memory with cp.async while the
 // current item's FFTs run (bin 1 only; rows of 4-byte aligned, 4-byte multiple length).
 template <int LOG2N, bool RAW, bool PREF>
-__global__ void __launch_bounds__(256, LOG2N >= 11 ? 1 : 2) fft_filter_kernel(Filter2Args A) {
+__global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A) {
     using P = fft::Plan<LOG2N>;
     constexpr int N = P::N, G = P::G, FPB = P::FPB;
     constexpr int ES = RAW ? 2 : 4;                      // input element size
