@@ -377,6 +377,25 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
             const uint32_t vmask = __ballot_sync(0xffffffffu, lane < RPW && ri.pix >= 0);
             const unsigned long long src0 = __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(ri.src), 0);
             const long long vstride = A.s_view * (RAW ? 2 : 4);          // bytes between views
+            if (fast && t + gridDim.x < n_tiles) {
+                // L2 prefetch of this warp's 16 input rows of the CTA's next tile (every 128-byte
+                // line of each row): their loads then come from L2 instead of DRAM
+                const long long tn = t + gridDim.x;
+                const int rn = (int)(tn % A.rows);
+                const int vbn = (int)(tn / A.rows);
+                const int rrn = (RAW && A.flip) ? (A.rows - 1 - rn) : rn;
+                const int lines = (A.cols * (RAW ? 2 : 4) + 127) / 128;
+                for (int e = lane; e < RPW * lines; e += 32) {
+                    const int i = e / lines, j = e - (e / lines) * lines;
+                    const int v = vbn * TILE_M + pw * RPW + i;
+                    if (v < A.k) {
+                        const unsigned char* pf = static_cast<const unsigned char*>(A.src) +
+                                                  ((long long)v * A.s_view + (long long)rrn * A.s_row) * (RAW ? 2 : 4) +
+                                                  128 * j;
+                        asm volatile("prefetch.global.L2 [%0];" ::"l"(pf));
+                    }
+                }
+            }
             if (fast) {
                 // software pipeline: the loads of K-blocks I + 1 and I + 2 are in flight while
                 // block I is converted (16 rows x 3 blocks of requests per warp)
