@@ -18,6 +18,7 @@ collective on the data path); value = all ranks' updates / max-over-ranks time.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -572,6 +573,73 @@ def run_reference(args, rank, world, local):
             "wall_s": wall}
 
 
+# ------------------------------------------------------------------ single-kernel cases
+def run_case(args):
+    """One kernel family on its own, device-timed with CUDA events (no host copies):
+    otsu        the three voxel passes of model.otsu_threshold on a 640^3 float32 volume
+    correct     the loaders' correction + crop (mr_correct_u16) of 120 views 1944 x 1536
+    ingest-full the fused FFT ingest of 1200 raw views 1944 x 1536 into a bf16 ring
+    Prints one JSON line: the case's own throughput and its HBM figure."""
+    import torch
+    from tomography_local_demo_b200 import SliceReconstructor, circular_cone_vectors
+    from tomography_local_demo_b200 import _native as N
+    from tomography_local_demo_b200.model import otsu_threshold
+    dev = torch.device("cuda", 0)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1)
+    if args.case == "otsu":
+        vol = torch.rand((640, 640, 640), generator=gen, device=dev) * 0.5
+        vol[vol < 0.05] = 0
+        step = lambda: otsu_threshold(vol)                        # noqa: E731 (waits for its result)
+        units, unit, nbytes = vol.numel(), "voxels/s", 5 * vol.numel() * 4     # 5 passes over the voxels
+    elif args.case == "correct":
+        k, R0, C0 = args.case_views or 120, 1536, 1944
+        raw = torch.randint(30000, 50000, (k, R0, C0), generator=gen, device=dev, dtype=torch.int32).to(torch.int16)
+        dark = torch.full((R0, C0), 100.0, device=dev)
+        gain = torch.full((R0, C0), 1.0 / 49900.0, device=dev)
+        out = torch.empty((R0, k, C0), device=dev)
+        lib, v = N.load(), ctypes.c_void_p
+
+        def step():
+            N.check(lib.mr_correct_u16(v(raw.data_ptr()), R0 * C0, C0, k, 1, 1, R0, 0, 0, R0, C0, v(dark.data_ptr()),
+                                       v(gain.data_ptr()), C0, N.MR_CORRECT_FLEXRAY, v(out.data_ptr()), k * C0, C0,
+                                       v(torch.cuda.current_stream().cuda_stream)), "mr_correct_u16")
+        units, unit, nbytes = k, "views/s", k * R0 * C0 * (2 + 4)
+    else:
+        V, R0, C0 = args.case_views or 1200, 1536, 1944
+        geom = circular_cone_vectors(V, 440.0, 680.0, R0, C0, 0.0748)
+        raw = torch.randint(30000, 50000, (V, R0, C0), generator=gen, device=dev, dtype=torch.int32).to(torch.int16)
+        rec = SliceReconstructor(None, geom, window="ram-lak", store="bf16", verbose=False, filter="fft")
+        rec.set_flat_dark(np.full((2, R0, C0), 50000, np.uint16), np.full((2, R0, C0), 100, np.uint16))
+        idx = np.arange(V)
+
+        def step():
+            rec.reset()
+            rec.add_raw_projections(idx, raw)
+            torch.cuda.current_stream().wait_stream(rec.ingest_stream)   # the timed stream sees it
+        units, unit, nbytes = V, "views/s", V * R0 * C0 * (2 + 2)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, source = float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        peak, source = 6650.0, "fallback"
+    gbs = nbytes / ms / 1e6
+    return {"case": args.case, "metric": unit.split("/")[0] + " per second", "value": units / ms * 1e3,
+            "unit": unit, "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+            "hbm": {"algorithmic_bytes": nbytes, "achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak,
+                    "peak_source": source}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -583,9 +651,15 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the live-scan serving simulation")
     ap.add_argument("--filter", choices=("fft", "tc", "tc-bf16"), default="tc",
                     help="row filter: shared-memory FFT or tensor-core Toeplitz GEMM (split FP16 / BF16)")
+    ap.add_argument("--case", choices=("otsu", "correct", "ingest-full"), default=None,
+                    help="time one other kernel family alone instead of the headline step")
+    ap.add_argument("--case-views", type=int, default=0, help="views of the correct / ingest-full case")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.case is not None:
+        print(json.dumps(run_case(args)), flush=True)
+        return
     rank, world, local = dist_setup()
     try:
         line = (run_reference if args.impl == "reference" else run_ours)(args, rank, world, local)
