@@ -254,6 +254,31 @@ int mr_ingest_u16(const uint16_t* raw, int64_t s_view, int64_t s_row,
                   const float* H_dev, const float* twiddle_dev, int32_t log2n,
                   const mr_ring* ring, void* stream);
 
+/* ---- iso-surface of a volume (marching cubes) -------------------------------------
+ * Replaces the contour step of model.py:40-69 (extract_surface: VTK flying edges, or
+ * scikit-image's marching cubes). vol: device f32 [nx][ny][nz] (z fastest), the grid point
+ * (i, j, k) at origin + spacing * (i, j, k); a corner is inside when its value > iso (NaN:
+ * outside). Cells are the (nx-1)(ny-1)(nz-1) cubes in memory order of their lowest corner,
+ * in blocks of 256. The case table is built by the library from the cube's geometry:
+ * table[16*m + 0..14] = three edge numbers per triangle of pattern m (-1 after the last),
+ * table[16*m + 15] = triangle count (<= 5); corners c = dx + 2 dy + 4 dz, edges 0-3 along
+ * x from the corners with dx = 0, 4-7 along y, 8-11 along z; normals point from inside
+ * to outside; a shared face is cut alike from both cells, so surfaces are closed. */
+int64_t mr_mc_blocks(int32_t nx, int32_t ny, int32_t nz);     /* blocks of 256 cells */
+int mr_mc_table(int8_t* table_host);                          /* 256 x 16 bytes, host only */
+/* block_counts: device int32 [mr_mc_blocks()], the triangles of each block. */
+int mr_mc_count(const float* vol, int32_t nx, int32_t ny, int32_t nz, float iso,
+                int32_t* block_counts_dev, void* stream);
+/* block_offsets: device int64, the exclusive prefix sums of block_counts; n_tri: their
+ * total (the capacity of the outputs). Per vertex v of triangle t (v = 3t + q):
+ * tri_edges[v] = grid edge id 3 * ((i*ny + j)*nz + k) + axis of the edge it lies on
+ * (identical for the cells sharing the edge), tri_pos[3v .. 3v+2] = its position,
+ * origin + spacing * (corner + s * axis), s = (iso - v_a) / (v_b - v_a), every FP32
+ * operation rounded on its own. origin: host, 3 doubles. */
+int mr_mc_emit(const float* vol, int32_t nx, int32_t ny, int32_t nz, float iso,
+               const double* origin, double spacing, const int64_t* block_offsets_dev,
+               int64_t n_tri, int64_t* tri_edges_dev, float* tri_pos_dev, void* stream);
+
 /* ---- raw correction alone (the scan loaders' output stack) ------------------------
  * Replaces the per-projection correction of flexray.py:111-116 + 174-184 (`corrected`,
  * mode MR_CORRECT_FLEXRAY: float32 bin mean, (mean - dark) * scale, scale = the gain

@@ -78,6 +78,11 @@ SIGNATURES = {
     "mr_slice_entropy": (ctypes.c_int, [_P, _I32, _I64, _I32, _I32, _P, _P]),
     "mr_correct_u16": (ctypes.c_int, [_P, _I64, _I64, _I32, _I32, _I32, _I32, _I32, _I32, _I32, _I32, _P, _P,
                                        _I64, _I32, _P, _I64, _I64, _P]),
+    "mr_mc_blocks": (_I64, [_I32, _I32, _I32]),
+    "mr_mc_table": (ctypes.c_int, [_P]),
+    "mr_mc_count": (ctypes.c_int, [_P, _I32, _I32, _I32, ctypes.c_float, _P, _P]),
+    "mr_mc_emit": (ctypes.c_int, [_P, _I32, _I32, _I32, ctypes.c_float, _P, ctypes.c_double, _P, _I64, _P, _P,
+                                  _P]),
     "mr_volume_workspace_bytes": (_I64, []),
     "mr_volume_stats": (ctypes.c_int, [_P, _I64, _P, _P, _P]),
     "mr_volume_select": (ctypes.c_int, [_P, _I64, _P, _I32, ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P]),
