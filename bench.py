@@ -577,6 +577,7 @@ def run_reference(args, rank, world, local):
 def run_case(args):
     """One kernel family on its own, device-timed with CUDA events (no host copies):
     otsu        the three voxel passes of model.otsu_threshold on a 640^3 float32 volume
+    surface     model.marching_cubes of a 640^3 float32 volume (a noisy ball of radius 250)
     correct     the loaders' correction + crop (mr_correct_u16) of 120 views 1944 x 1536
     ingest-full the fused FFT ingest of 1200 raw views 1944 x 1536 into a bf16 ring
     Prints one JSON line: the case's own throughput and its HBM figure."""
@@ -592,6 +593,13 @@ def run_case(args):
         vol[vol < 0.05] = 0
         step = lambda: otsu_threshold(vol)                        # noqa: E731 (waits for its result)
         units, unit, nbytes = vol.numel(), "voxels/s", 5 * vol.numel() * 4     # 5 passes over the voxels
+    elif args.case == "surface":
+        from tomography_local_demo_b200.model import marching_cubes
+        x = torch.arange(640, device=dev, dtype=torch.float32) - 319.5
+        vol = 250.0 - torch.sqrt(x[:, None, None] ** 2 + x[None, :, None] ** 2 + x[None, None, :] ** 2)
+        vol += 0.3 * torch.randn(vol.shape, generator=gen, device=dev)
+        step = lambda: marching_cubes(vol, 0.0, (0.0, 0.0, 0.0), 0.0825)   # noqa: E731
+        units, unit, nbytes = vol.numel(), "voxels/s", 2 * vol.numel() * 4     # two passes over the voxels
     elif args.case == "correct":
         k, R0, C0 = args.case_views or 120, 1536, 1944
         raw = torch.randint(30000, 50000, (k, R0, C0), generator=gen, device=dev, dtype=torch.int32).to(torch.int16)
@@ -651,7 +659,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the live-scan serving simulation")
     ap.add_argument("--filter", choices=("fft", "tc", "tc-bf16"), default="tc",
                     help="row filter: shared-memory FFT or tensor-core Toeplitz GEMM (split FP16 / BF16)")
-    ap.add_argument("--case", choices=("otsu", "correct", "ingest-full"), default=None,
+    ap.add_argument("--case", choices=("otsu", "surface", "correct", "ingest-full"), default=None,
                     help="time one other kernel family alone instead of the headline step")
     ap.add_argument("--case-views", type=int, default=0, help="views of the correct / ingest-full case")
     args = ap.parse_args()

@@ -259,12 +259,12 @@ int mr_ingest_u16(const uint16_t* raw, int64_t s_view, int64_t s_row,
  * scikit-image's marching cubes). vol: device f32 [nx][ny][nz] (z fastest), the grid point
  * (i, j, k) at origin + spacing * (i, j, k); a corner is inside when its value > iso (NaN:
  * outside). Cells are the (nx-1)(ny-1)(nz-1) cubes in memory order of their lowest corner,
- * in blocks of 256. The case table is built by the library from the cube's geometry:
+ * in blocks of up to 256 cells of one z row (nx, ny <= 65536). The case table is built by the library from the cube's geometry:
  * table[16*m + 0..14] = three edge numbers per triangle of pattern m (-1 after the last),
  * table[16*m + 15] = triangle count (<= 5); corners c = dx + 2 dy + 4 dz, edges 0-3 along
  * x from the corners with dx = 0, 4-7 along y, 8-11 along z; normals point from inside
  * to outside; a shared face is cut alike from both cells, so surfaces are closed. */
-int64_t mr_mc_blocks(int32_t nx, int32_t ny, int32_t nz);     /* blocks of 256 cells */
+int64_t mr_mc_blocks(int32_t nx, int32_t ny, int32_t nz);     /* (nx-1)(ny-1)ceil((nz-1)/256) */
 int mr_mc_table(int8_t* table_host);                          /* 256 x 16 bytes, host only */
 /* block_counts: device int32 [mr_mc_blocks()], the triangles of each block. */
 int mr_mc_count(const float* vol, int32_t nx, int32_t ny, int32_t nz, float iso,

@@ -1,7 +1,8 @@
 // Iso-surface of a reconstructed volume by marching cubes: the contour step of minirecast
 // model.py:40-69 (extract_surface), which the reference hands to VTK's flying edges (or
 // scikit-image). Two passes over the cells of a float32 volume [nx][ny][nz] (z fastest):
-//   mr_mc_count  triangles per block of 256 cells (the host scans these into offsets)
+//   mr_mc_count  triangles per block of up to 256 cells of one z row (the host scans these
+//                into offsets)
 //   mr_mc_emit   each cell's triangles at its block's offset + its rank inside the block:
 //                per vertex the grid edge it lies on (for sharing vertices between cells)
 //                and its position, interpolated in FP32 along the edge
@@ -150,37 +151,41 @@ static int ensure_table() {
 struct McArgs {
     const float* vol;
     int nx, ny, nz;
+    int kchunks;                                // blocks of 256 cells along z per (i, j) row
     long long cells;
     float iso;
     float ox, oy, oz, h;
 };
 
-// Case of cell `cell` (cells in memory order of their lowest corner, z fastest).
-__device__ __forceinline__ int cell_case(const McArgs& g, long long cell, int& i, int& j, int& k, float val[8]) {
-    const int ck = g.nz - 1, cj = g.ny - 1;
-    k = (int)(cell % ck);
-    const long long r = cell / ck;
-    j = (int)(r % cj);
-    i = (int)(r / cj);
+// Cell (i, j, k) of this thread: blocks run over rows of cells along z (blockIdx.x: 256-cell
+// chunk of the row, blockIdx.y: j, blockIdx.z: i), so block order is cell memory order.
+// Returns the case of the cell, or -1 past the row's end.
+__device__ __forceinline__ int cell_case(const McArgs& g, int& i, int& j, int& k, float val[8]) {
+    i = blockIdx.z;
+    j = blockIdx.y;
+    k = blockIdx.x * MC_THREADS + threadIdx.x;
+    if (k >= g.nz - 1) return -1;
+    const float* p = g.vol + ((long long)i * g.ny + j) * g.nz + k;
+    const long long sx = (long long)g.ny * g.nz, sy = g.nz;
     int m = 0;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        const long long idx = ((long long)(i + (c & 1)) * g.ny + (j + ((c >> 1) & 1))) * g.nz + (k + ((c >> 2) & 1));
-        val[c] = __ldg(g.vol + idx);
+        val[c] = __ldg(p + (c & 1) * sx + ((c >> 1) & 1) * sy + ((c >> 2) & 1));
         m |= (val[c] > g.iso ? 1 : 0) << c;
     }
     return m;
 }
 
+__device__ __forceinline__ long long block_id(const McArgs& g) {
+    return ((long long)blockIdx.z * gridDim.y + blockIdx.y) * g.kchunks + blockIdx.x;
+}
+
 __global__ void __launch_bounds__(MC_THREADS) mc_count_kernel(McArgs g, int* __restrict__ block_counts) {
     __shared__ int warp_sum[MC_THREADS / 32];
-    const long long cell = (long long)blockIdx.x * MC_THREADS + threadIdx.x;
-    int cnt = 0;
-    if (cell < g.cells) {
-        int i, j, k;
-        float val[8];
-        cnt = c_mc_tri[cell_case(g, cell, i, j, k, val)][15];
-    }
+    int i, j, k;
+    float val[8];
+    const int m = cell_case(g, i, j, k, val);
+    int cnt = m >= 0 ? c_mc_tri[m][15] : 0;
 #pragma unroll
     for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = cnt;
@@ -188,7 +193,7 @@ __global__ void __launch_bounds__(MC_THREADS) mc_count_kernel(McArgs g, int* __r
     if (threadIdx.x == 0) {
         int s = 0;
         for (int w = 0; w < MC_THREADS / 32; ++w) s += warp_sum[w];
-        block_counts[blockIdx.x] = s;
+        block_counts[block_id(g)] = s;
     }
 }
 
@@ -196,14 +201,11 @@ __global__ void __launch_bounds__(MC_THREADS)
 mc_emit_kernel(McArgs g, const long long* __restrict__ block_offsets, long long n_tri,
                long long* __restrict__ tri_edges, float* __restrict__ tri_pos) {
     __shared__ int warp_sum[MC_THREADS / 32];
-    const long long cell = (long long)blockIdx.x * MC_THREADS + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int i = 0, j = 0, k = 0, m = 0, cnt = 0;
+    int i, j, k;
     float val[8];
-    if (cell < g.cells) {
-        m = cell_case(g, cell, i, j, k, val);
-        cnt = c_mc_tri[m][15];
-    }
+    const int m = cell_case(g, i, j, k, val);
+    const int cnt = m >= 0 ? c_mc_tri[m][15] : 0;
     // exclusive rank of this cell's triangles inside the block
     int incl = cnt;
 #pragma unroll
@@ -215,7 +217,7 @@ mc_emit_kernel(McArgs g, const long long* __restrict__ block_offsets, long long 
     __syncthreads();
     int before = 0;
     for (int w = 0; w < warp; ++w) before += warp_sum[w];
-    const long long first = block_offsets[blockIdx.x] + before + incl - cnt;
+    const long long first = block_offsets[block_id(g)] + before + incl - cnt;
     for (int t = 0; t < cnt; ++t) {
         const long long o = first + t;
         if (o >= n_tri) break;                          // never write past the caller's buffers
@@ -243,22 +245,24 @@ mc_emit_kernel(McArgs g, const long long* __restrict__ block_offsets, long long 
 static int fill_args(McArgs& g, const float* vol, int32_t nx, int32_t ny, int32_t nz, float iso) {
     if (!vol || nx < 2 || ny < 2 || nz < 2 || !(iso == iso)) return MR_ERR_INVALID;
     if (((uintptr_t)vol & 3u)) return MR_ERR_INVALID;
+    if (nx - 1 > 65535 || ny - 1 > 65535) return MR_ERR_UNSUPPORTED;     // grid y / z limits
     g.vol = vol;
     g.nx = nx;
     g.ny = ny;
     g.nz = nz;
+    g.kchunks = (nz - 1 + MC_THREADS - 1) / MC_THREADS;
     g.cells = (long long)(nx - 1) * (ny - 1) * (nz - 1);
     g.iso = iso;
-    if ((g.cells + MC_THREADS - 1) / MC_THREADS > 2147483647LL) return MR_ERR_UNSUPPORTED;
     return MR_OK;
 }
+
+static dim3 mc_grid(const McArgs& g) { return dim3((unsigned)g.kchunks, (unsigned)(g.ny - 1), (unsigned)(g.nx - 1)); }
 
 }  // namespace mr
 
 extern "C" int64_t mr_mc_blocks(int32_t nx, int32_t ny, int32_t nz) {
     if (nx < 2 || ny < 2 || nz < 2) return 0;
-    const long long cells = (long long)(nx - 1) * (ny - 1) * (nz - 1);
-    return (cells + mr::MC_THREADS - 1) / mr::MC_THREADS;
+    return (int64_t)(nx - 1) * (ny - 1) * ((nz - 1 + mr::MC_THREADS - 1) / mr::MC_THREADS);
 }
 
 extern "C" int mr_mc_table(int8_t* table_host) {
@@ -277,8 +281,7 @@ extern "C" int mr_mc_count(const float* vol, int32_t nx, int32_t ny, int32_t nz,
     if (!block_counts) return MR_ERR_INVALID;
     rc = mr::ensure_table();
     if (rc != MR_OK) return rc;
-    const long long blocks = (g.cells + mr::MC_THREADS - 1) / mr::MC_THREADS;
-    mr::mc_count_kernel<<<(unsigned)blocks, mr::MC_THREADS, 0, static_cast<cudaStream_t>(stream)>>>(g, block_counts);
+    mr::mc_count_kernel<<<mr::mc_grid(g), mr::MC_THREADS, 0, static_cast<cudaStream_t>(stream)>>>(g, block_counts);
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;
 }
@@ -297,8 +300,7 @@ extern "C" int mr_mc_emit(const float* vol, int32_t nx, int32_t ny, int32_t nz, 
     g.oy = (float)origin[1];
     g.oz = (float)origin[2];
     g.h = (float)spacing;
-    const long long blocks = (g.cells + mr::MC_THREADS - 1) / mr::MC_THREADS;
-    mr::mc_emit_kernel<<<(unsigned)blocks, mr::MC_THREADS, 0, static_cast<cudaStream_t>(stream)>>>(
+    mr::mc_emit_kernel<<<mr::mc_grid(g), mr::MC_THREADS, 0, static_cast<cudaStream_t>(stream)>>>(
         g, reinterpret_cast<const long long*>(block_offsets), (long long)n_tri,
         reinterpret_cast<long long*>(tri_edges), tri_pos);
     MR_CUDA_TRY(cudaGetLastError());
