@@ -88,8 +88,8 @@ def as_u16(t):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """Samples SM clock, power and clock-event reasons every 10 ms during the timed
-    region through NVML (read-only queries; nothing is set)."""
+    """Samples SM clock, power and clock-event reasons every 2 ms during the timed region
+    and once at its end, through NVML (read-only queries; nothing is set)."""
     BITS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
             "sw_power_cap": 0x4}
 
@@ -110,29 +110,45 @@ class ClockSampler:
             idx = int(vis.split(",")[self.dev]) if vis and vis.split(",")[0].isdigit() else self.dev
             return nv.nvmlDeviceGetHandleByIndex(idx)
 
+    def _sample(self):
+        nv, h = self._nv, self._h
+        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                             int(self._reasons(h)), nv.nvmlDeviceGetPowerUsage(h) / 1e3))
+
     def _run(self):
         try:
-            import pynvml as nv
-            nv.nvmlInit()
-            h = self._handle(nv)
-            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
-            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
-                nv.nvmlDeviceGetCurrentClocksThrottleReasons
-            while not self._stop.is_set():
-                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
-                                     int(get_reasons(h)), nv.nvmlDeviceGetPowerUsage(h) / 1e3))
-                self._stop.wait(0.01)
-        except Exception as e:             # no NVML: report unsampled
+            while True:
+                self._sample()
+                if self._stop.wait(0.002):
+                    break
+        except Exception as e:
             self.error = repr(e)
 
     def __enter__(self):
-        self.thread = threading.Thread(target=self._run, daemon=True)
+        # NVML is opened before the timed region, so sampling starts with it
+        self._nv = None
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self._h = self._handle(nv)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self._h, nv.NVML_CLOCK_SM))
+            self._reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self._nv = nv
+        except Exception as e:             # no NVML: report unsampled
+            self.error = repr(e)
+        self.thread = threading.Thread(target=self._run if self._nv else (lambda: None), daemon=True)
         self.thread.start()
         return self
 
     def __exit__(self, *a):
         self._stop.set()
         self.thread.join(5)
+        if self._nv is not None:
+            try:
+                self._sample()             # one more right at the end of the timed region
+            except Exception as e:
+                self.error = repr(e)
 
     def summary(self):
         if not self.samples:
