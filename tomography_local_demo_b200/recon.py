@@ -149,6 +149,49 @@ def parallel_view_maps(angles, pixel_u, pixel_v, rows, cols, qscale=None):
     return out
 
 
+def parker_weights(vectors, cols):
+    """Short-scan weights w[v, c] of D. L. Parker (Med. Phys. 9, 254-257, 1982) for a circular
+    cone-beam orbit, FP64 [views, cols].
+
+    beta = source angle from the first view along the orbit, gamma = fan angle of column c
+    in the mid-plane, measured from the central ray (source -> rotation axis) in the
+    direction of rotation, so that the ray (beta, gamma) is measured again at
+    (beta + pi + 2 gamma, -gamma). With 2 delta = (last beta) - pi:
+      w = sin^2(pi/4 * beta / (delta - gamma))               0 <= beta < 2 (delta - gamma)
+      w = 1                                                   up to beta = pi - 2 gamma
+      w = sin^2(pi/4 * (pi + 2 delta - beta) / (delta + gamma))  up to beta = pi + 2 delta
+    so that every ray's two measurements weigh 1 together. The weights are multiplied by
+    n d_beta / pi, which keeps the back-projection's FDK scale pi / n right for the weighted
+    short scan (a full scan has no such scale: each ray counts twice with weight 1 / 2)."""
+    V = np.asarray(vectors, dtype=np.float64)
+    n = len(V)
+    if n < 3:
+        raise ValueError("Parker weights need at least 3 views")
+    s, d, u = V[:, 0:3], V[:, 3:6], V[:, 6:9]
+    th = np.unwrap(np.arctan2(s[:, 1], s[:, 0]))
+    sigma = 1.0 if th[-1] >= th[0] else -1.0
+    beta = sigma * (th - th[0])
+    d_beta = beta[-1] / (n - 1)
+    if beta[-1] + 1.5 * d_beta >= 2 * np.pi:
+        raise ValueError("Parker weights are for short scans: this orbit covers a full turn")
+    off = np.arange(cols) - (cols - 1) / 2.0
+    ray = d[:, None, :] + off[None, :, None] * u[:, None, :] - s[:, None, :]       # [n, C, 3]
+    cen = -s
+    gamma = sigma * np.arctan2(cen[:, None, 0] * ray[..., 1] - cen[:, None, 1] * ray[..., 0],
+                               cen[:, None, 0] * ray[..., 0] + cen[:, None, 1] * ray[..., 1])
+    delta = (beta[-1] - np.pi) / 2.0
+    if delta <= np.abs(gamma).max():
+        raise ValueError(f"the orbit covers {np.degrees(beta[-1]):.1f} deg: a short scan needs 180 deg "
+                         f"plus the fan angle ({np.degrees(2 * np.abs(gamma).max()):.1f} deg)")
+    b = beta[:, None]
+    w = np.ones_like(gamma)
+    lo = b < 2.0 * (delta - gamma)
+    hi = b > np.pi - 2.0 * gamma
+    w[lo] = np.sin(np.pi / 4.0 * (b / (delta - gamma))[lo]) ** 2
+    w[hi] = np.sin(np.pi / 4.0 * ((np.pi + 2.0 * delta - b) / (delta + gamma))[hi]) ** 2
+    return w * (n * d_beta / np.pi)
+
+
 def cone_filter_views(K, rows, cols, n_fft, slots, out_scale=1.0):
     """mr_filter_view records of cone views (fdk_filter_block, recon.py:93-103)."""
     s, d, u, v, n = K["s"], K["d"], K["u"], K["v"], K["n"]
@@ -486,13 +529,16 @@ class SliceReconstructor:
                cores, split FP16 operands, FP32 accumulation; rows <= 512 columns) or
                "tc-bf16" (the same with split BF16 operands, ~100x less precise on
                smooth rows because the ramp filter cancels strongly).
+    parker   : weight a cone-beam short scan (180 deg plus the fan angle, up to a full turn)
+               with Parker's weights before the filter; the reference has no such weights
+               and only warns (recon.py:331-332).
     The `backend` argument is accepted for compatibility; the backend is always
     "cuda-sm100a".
     """
 
     def __init__(self, proj=None, geom=None, window="shepp-logan", backend="auto",
                  gaussian=0.0, tilt=0.0, verbose=True, store="fp32", device=None, filter="fft",
-                 keep_projections=False):
+                 keep_projections=False, parker=False):
         if geom is None:
             raise ValueError("geometry is required")
         if store not in _STORE_DTYPES:
@@ -534,7 +580,7 @@ class SliceReconstructor:
             self._kind_code = N.MR_CONE
             self._K_all = cone_constants(geom.vectors)
             self._maps_all = cone_view_maps(self._K_all, R, C)
-            if geom.angular_range < 2 * np.pi - 1e-3 and verbose:
+            if geom.angular_range < 2 * np.pi - 1e-3 and verbose and not parker:
                 print("note: short scan (<360 deg) - no Parker weights, expect some artefacts")
         else:
             raise TypeError(type(geom))
@@ -550,6 +596,12 @@ class SliceReconstructor:
             self._views_dev = torch.zeros(self.n_total * N.VIEW_DTYPE.itemsize, dtype=torch.uint8,
                                           device=self.device)
         self._ring_c = _ring_struct(self._ring, self._dtype_code, self._kind_code, R, C)
+        self._parker = None             # [n_total, C] f32 short-scan weights (device)
+        if parker:
+            if self.kind != "cone":
+                raise ValueError("Parker weights apply to cone-beam orbits")
+            with torch.cuda.device(self.device):
+                self._parker = torch.from_numpy(parker_weights(geom.vectors, C).astype(np.float32)).to(self.device)
         self._proj = None               # unfiltered line integrals [n_total, R, pitch] (keep_projections)
         if keep_projections:
             with torch.cuda.device(self.device):
@@ -636,6 +688,12 @@ class SliceReconstructor:
                 x, s_view, s_row = preprocess.apply_device(x, self.gaussian, self.tilt)
                 if self._proj is not None:
                     self._proj[n0:n0 + k, :, :C] = torch.as_strided(x, (k, R, C), (s_view, s_row, 1))
+                if self._parker is not None:
+                    # short-scan weights on a copy (x may be the caller's own tensor)
+                    w = self._parker[torch.from_numpy(indices).to(self.device)]          # [k, C]
+                    xw = torch.empty((k, R, C), dtype=torch.float32, device=self.device)
+                    torch.mul(torch.as_strided(x, (k, R, C), (s_view, s_row, 1)), w[:, None, :], out=xw)
+                    x, s_view, s_row = xw, R * C, C
                 fv = _struct_tensor(self._filter_views(indices, slots), self.device)
                 filter_block_device(x, s_view, s_row, k, fv, self._tables, self._ring_c,
                                     self.ingest_stream, self.filter_method, self._status)
@@ -705,6 +763,10 @@ class SliceReconstructor:
         if raw.shape[1] < R * b or raw.shape[2] < C * b:
             raise ValueError(f"raw frames {tuple(raw.shape[1:])} are smaller than "
                              f"{R * b} x {C * b}")
+        if self._parker is not None:
+            # short scan: the Parker weights go between the correction and the filter, so
+            # the counts are corrected on their own (mr_correct_u16) and filtered as a block
+            return self.add_projections(indices, self._correct_raw(raw))
         with self._ingest_lock:
             keep = ~self._received[indices]
             if not keep.all():
@@ -743,6 +805,33 @@ class SliceReconstructor:
                     marks = [(n0 + c1, e) for c1, e in self._ingest_host(raw, k, prepare)[:-1]]
                 ev = torch.cuda.Event()
             return self._admit(indices, slots, ev, uploaded=True, marks=marks)
+
+    def _correct_raw(self, raw):
+        """Line integrals [rows, k, cols] f32 (device) of raw counts [k, R0, C0]: the
+        correction of the fused ingest (bin, row flip, (P-D)*gain, clip, -log) alone."""
+        R, C, b = self.geom.rows, self.geom.cols, self._raw_bin
+        with torch.cuda.device(self.device), torch.cuda.stream(self.ingest_stream):
+            if isinstance(raw, torch.Tensor):
+                t = raw.view(torch.int16) if raw.dtype == torch.uint16 else raw
+                if t.element_size() != 2:
+                    raise ValueError("raw counts must be 16-bit")
+            else:
+                arr = np.asarray(raw)
+                if arr.dtype.itemsize != 2:
+                    raise ValueError("raw counts must be 16-bit")
+                t = torch.from_numpy(np.ascontiguousarray(arr).view(np.int16))
+            t = t.to(self.device, non_blocking=True).contiguous()
+            k, R0, C0 = t.shape
+            out = torch.empty((R, k, C), dtype=torch.float32, device=self.device)
+            for v0 in range(0, k, 65535):
+                v1 = min(k, v0 + 65535)
+                N.check(N.load().mr_correct_u16(ctypes_void(t[v0].data_ptr()), R0 * C0, C0, v1 - v0, b,
+                                                int(self._raw_flip), R, 0, 0, R, C, ctypes_void(self._dark.data_ptr()),
+                                                ctypes_void(self._gain.data_ptr()), C, N.MR_CORRECT_FLEXRAY,
+                                                ctypes_void(out[:, v0].data_ptr()), k * C, C,
+                                                ctypes_void(self.ingest_stream.cuda_stream)), "mr_correct_u16")
+            t.record_stream(self.ingest_stream)
+        return out
 
     def _keep_raw_line_integrals(self, raw, n0, k):
         """-log(max((binned counts - dark) * gain, 1e-3)) of k raw views into the kept
