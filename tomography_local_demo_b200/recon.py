@@ -330,23 +330,30 @@ class KernelTimer:
 
 
 def backproject_device(ring, views_dev, grids, out, stream, device, timer=None, kernel="staged",
-                       status=None):
+                       status=None, wait=None):
     """Back-project numpy GRID_DTYPE records into the device f32 tensor `out`.
 
     kernel="staged": regular grids go through mr_backproject_staged (TMA-staged
     footprints); point lists always use mr_backproject. kernel="plain": everything uses
-    mr_backproject (direct global gathers) - the plain GPU path kept for comparison."""
+    mr_backproject (direct global gathers) - the plain GPU path kept for comparison.
+    wait: an event the launch must follow (the filter of the views summed); the grid and
+    tile records are uploaded before the stream waits for it."""
     grids = np.ascontiguousarray(grids, dtype=N.GRID_DTYPE)
     is_pts = (grids["flags"] & N.MR_GRID_POINTS) != 0
     if kernel == "staged" and is_pts.any() and not is_pts.all():
-        backproject_device(ring, views_dev, grids[is_pts], out, stream, device, timer, "plain")
+        backproject_device(ring, views_dev, grids[is_pts], out, stream, device, timer, "plain", wait=wait)
+        wait = None
         grids = grids[~is_pts]
         is_pts = is_pts[~is_pts]
     tiles = N.plan_tiles(grids)
     if len(tiles) == 0:
+        if wait is not None:
+            stream.wait_event(wait)
         return
     g_dev = _struct_tensor(grids, device)
     t_dev = _struct_tensor(tiles, device)
+    if wait is not None:
+        stream.wait_event(wait)
     lib = N.load()
     v = ctypes_void
     staged = kernel == "staged" and not is_pts.any()
@@ -1068,12 +1075,10 @@ class SliceReconstructor:
                 g_dev.record_stream(stream)
                 t_dev.record_stream(stream)
             return
-        if event is not None:
-            stream.wait_event(event)
         grids["n_views"] = n
         with torch.cuda.device(self.device), torch.cuda.stream(stream):
             backproject_device(self._ring_c, self._views_dev, grids, out, stream, self.device,
-                               self.kernel_timer, self.bp_kernel, self._status)
+                               self.kernel_timer, self.bp_kernel, self._status, wait=event)
 
     def reconstruct_points_tensor(self, pts, cor_shift=None):
         """Device variant of reconstruct_points: pts (M, 3) -> f32 tensor [M]."""
