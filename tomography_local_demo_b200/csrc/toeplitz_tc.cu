@@ -18,7 +18,7 @@
 //     bits (~1e-5 relative error of the filtered row), BF16 hi+lo 16 bits (~5e-4). FP16
 //     operands are scaled by powers of two into range: g by `t_scale` (max |g| t_scale in
 //     [2^13, 2^14)), the inputs by `x_scale`; the epilogue divides both out.
-//   * producer warps read the inputs (raw uint16 counts with flat/dark correction and
+//   * 16 producer warps read the inputs (raw uint16 counts with flat/dark correction and
 //     -log, or FP32 rows), apply the FDK cosine weight, split them and write them into a
 //     2-stage ring of SWIZZLE_128B K-major tiles; one thread issues tcgen05.mma (M = 128,
 //     N <= 256, K = 16) into an FP32 accumulator of KB * 64 columns in tensor memory; four
@@ -40,7 +40,9 @@ constexpr int TILE_M = 128;
 constexpr int KB_MAX = 8;                       // C <= 512
 constexpr int EPI_WARPS = 4;                    // warps 0..3 (TMEM lane quarters)
 constexpr int MMA_WARP = 4;
-constexpr int PROD_WARPS = 8;                   // warps 5..12
+constexpr int PROD_WARPS = 16;                  // warps 5..20: 8 rows (views) each; the
+                                                // conversion is latency-bound, so more warps
+                                                // (80 registers a thread) beat fewer, larger ones
 constexpr int THREADS = 32 * (EPI_WARPS + 1 + PROD_WARPS);
 constexpr int BLOCK_BYTES = 64 * 64 * 2;        // one 64 x 64 block of 16-bit values (8 KB)
 constexpr int A_TILE_BYTES = TILE_M * 128;      // 128 rows x 64 values (16 KB)
@@ -333,7 +335,7 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
     if (warp >= MMA_WARP + 1) {
         // ---------------- producers: inputs -> FDK weight -> 16-bit hi/lo -> swizzled tiles
         const int pw = warp - (MMA_WARP + 1);
-        constexpr int RPW = TILE_M / PROD_WARPS;                        // 16 rows (views) per warp
+        constexpr int RPW = TILE_M / PROD_WARPS;                        // rows (views) per warp
         RowInfo* my_rows = rows + pw * RPW;                             // read by this warp only
         // vector path: a lane's column pair is one aligned 4-byte (raw) / 8-byte (FP32) load
         const bool fast = RAW ? (A.bin == 1 && A.vec_src && A.vec_fld) : (A.vec_src && (A.cols % 2 == 0));
