@@ -269,10 +269,14 @@ def _handoff(stream, *tensors):
             t.record_stream(cur)
 
 
-def _struct_tensor(records, device):
-    """Device copy of numpy ABI records (a small pageable copy on the current stream: it is
-    not queued behind large pinned transfers that other streams have in flight)."""
+def _struct_tensor(records, device, asynchronous=False):
+    """Device copy of numpy ABI records on the current stream. By default a small pageable
+    copy, which the host waits for but which is not queued behind large pinned transfers
+    that other streams have in flight; asynchronous=True stages it in page-locked memory
+    instead, so the host does not wait (for when no such transfer is in flight)."""
     raw = np.ascontiguousarray(records).view(np.uint8)
+    if asynchronous:
+        return torch.from_numpy(raw.copy()).pin_memory().to(device, non_blocking=True)
     return torch.from_numpy(raw.copy()).to(device, non_blocking=False)
 
 
@@ -330,18 +334,20 @@ class KernelTimer:
 
 
 def backproject_device(ring, views_dev, grids, out, stream, device, timer=None, kernel="staged",
-                       status=None, wait=None):
+                       status=None, wait=None, asynchronous=False):
     """Back-project numpy GRID_DTYPE records into the device f32 tensor `out`.
 
     kernel="staged": regular grids go through mr_backproject_staged (TMA-staged
     footprints); point lists always use mr_backproject. kernel="plain": everything uses
     mr_backproject (direct global gathers) - the plain GPU path kept for comparison.
     wait: an event the launch must follow (the filter of the views summed); the grid and
-    tile records are uploaded before the stream waits for it."""
+    tile records are uploaded before the stream waits for it (asynchronously from
+    page-locked memory with asynchronous=True)."""
     grids = np.ascontiguousarray(grids, dtype=N.GRID_DTYPE)
     is_pts = (grids["flags"] & N.MR_GRID_POINTS) != 0
     if kernel == "staged" and is_pts.any() and not is_pts.all():
-        backproject_device(ring, views_dev, grids[is_pts], out, stream, device, timer, "plain", wait=wait)
+        backproject_device(ring, views_dev, grids[is_pts], out, stream, device, timer, "plain", wait=wait,
+                           asynchronous=asynchronous)
         wait = None
         grids = grids[~is_pts]
         is_pts = is_pts[~is_pts]
@@ -350,8 +356,8 @@ def backproject_device(ring, views_dev, grids, out, stream, device, timer=None, 
         if wait is not None:
             stream.wait_event(wait)
         return
-    g_dev = _struct_tensor(grids, device)
-    t_dev = _struct_tensor(tiles, device)
+    g_dev = _struct_tensor(grids, device, asynchronous)
+    t_dev = _struct_tensor(tiles, device, asynchronous)
     if wait is not None:
         stream.wait_event(wait)
     lib = N.load()
@@ -441,8 +447,8 @@ def plane_points(origin, normal, size, n):
     return np.asarray(origin, float) + a[..., None] * e1 + b[..., None] * e2
 
 
-def plane_size_for_box(box, normal):
-    _, e1, e2 = plane_basis(normal)
+def plane_size_for_box(box, normal, basis=None):
+    _, e1, e2 = plane_basis(normal) if basis is None else basis
     return 2.0 * float(max(np.abs(e1) @ box, np.abs(e2) @ box))
 
 
@@ -452,10 +458,10 @@ def _plane_frame(box, origin, normal, n, size, zoom, center):
     o = np.asarray(origin, float)
     c = np.zeros(3) if center is None else np.asarray(center, float)
     o = c - ((c - o) @ n_hat) * n_hat
+    basis = plane_basis(normal)
     if size is None:
-        size = plane_size_for_box(box, normal) / max(float(zoom), 1e-6)
-    _, e1, e2 = plane_basis(normal)
-    return o, e1, e2, float(size)
+        size = plane_size_for_box(box, normal, basis) / max(float(zoom), 1e-6)
+    return o, basis[1], basis[2], float(size)
 
 
 def slice_points(box, origin, normal, n=256, size=None, zoom=1.0, center=None):
@@ -1077,8 +1083,11 @@ class SliceReconstructor:
             return
         grids["n_views"] = n
         with torch.cuda.device(self.device), torch.cuda.stream(stream):
+            # no chunked host upload in flight (it would sit ahead of a page-locked copy on
+            # the copy engines): the records go up without the host waiting
             backproject_device(self._ring_c, self._views_dev, grids, out, stream, self.device,
-                               self.kernel_timer, self.bp_kernel, self._status, wait=event)
+                               self.kernel_timer, self.bp_kernel, self._status, wait=event,
+                               asynchronous=not self._chunk_marks)
 
     def reconstruct_points_tensor(self, pts, cor_shift=None):
         """Device variant of reconstruct_points: pts (M, 3) -> f32 tensor [M]."""
