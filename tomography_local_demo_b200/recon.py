@@ -356,8 +356,10 @@ def backproject_device(ring, views_dev, grids, out, stream, device, timer=None, 
         if wait is not None:
             stream.wait_event(wait)
         return
-    g_dev = _struct_tensor(grids, device, asynchronous)
-    t_dev = _struct_tensor(tiles, device, asynchronous)
+    # grid and tile records in one upload (the grid records are 256 bytes each, so the
+    # tiles that follow them stay aligned)
+    recs = _struct_tensor(np.concatenate([grids.view(np.uint8), tiles.view(np.uint8)]), device, asynchronous)
+    g_ptr, t_ptr = recs.data_ptr(), recs.data_ptr() + grids.nbytes
     if wait is not None:
         stream.wait_event(wait)
     lib = N.load()
@@ -366,19 +368,18 @@ def backproject_device(ring, views_dev, grids, out, stream, device, timer=None, 
     name = "mr_backproject_staged" if staged else "mr_backproject"
     ev0 = timer.start(stream) if timer is not None else None
     if staged:
-        st = lib.mr_backproject_staged(ring, v(views_dev.data_ptr()), v(g_dev.data_ptr()), v(t_dev.data_ptr()),
+        st = lib.mr_backproject_staged(ring, v(views_dev.data_ptr()), v(g_ptr), v(t_ptr),
                                        len(tiles), v(out.data_ptr()),
                                        v(status.data_ptr()) if status is not None else None,
                                        v(stream.cuda_stream))
     else:
-        st = lib.mr_backproject(ring, v(views_dev.data_ptr()), v(g_dev.data_ptr()), v(t_dev.data_ptr()),
+        st = lib.mr_backproject(ring, v(views_dev.data_ptr()), v(g_ptr), v(t_ptr),
                                 len(tiles), v(out.data_ptr()), v(stream.cuda_stream))
     if timer is not None:
         timer.stop(name, ev0, stream)
     N.check(st, name)
-    # keep the descriptor tensors alive until the kernel has consumed them
-    g_dev.record_stream(stream)
-    t_dev.record_stream(stream)
+    # keep the descriptor tensor alive until the kernel has consumed it
+    recs.record_stream(stream)
 
 
 # --------------------------------------------------------------------------
@@ -430,13 +431,21 @@ def fdk_filter_block(block, K, window="shepp-logan"):
 # --------------------------------------------------------------------------
 # Plane helpers (host, FP64) - recon.py:225-283
 # --------------------------------------------------------------------------
+def _cross3(a, b):
+    """a x b of two 3-vectors with numpy.cross's arithmetic (each component one product
+    minus another, rounded the same way) at a fraction of its call overhead."""
+    a0, a1, a2 = float(a[0]), float(a[1]), float(a[2])
+    b0, b1, b2 = float(b[0]), float(b[1]), float(b[2])
+    return np.array([a1 * b2 - a2 * b1, a2 * b0 - a0 * b2, a0 * b1 - a1 * b0])
+
+
 def plane_basis(normal):
     n = np.asarray(normal, dtype=float)
     n = n / np.linalg.norm(n)
     z = np.array([0.0, 0.0, 1.0])
-    e1 = np.cross(z, n) if abs(n @ z) < 0.9 else np.cross(n, np.array([0.0, 1.0, 0.0]))
+    e1 = _cross3(z, n) if abs(n @ z) < 0.9 else _cross3(n, (0.0, 1.0, 0.0))
     e1 /= np.linalg.norm(e1)
-    return n, e1, np.cross(n, e1)
+    return n, e1, _cross3(n, e1)
 
 
 def plane_points(origin, normal, size, n):
@@ -604,6 +613,13 @@ class SliceReconstructor:
             self.ingest_stream = torch.cuda.Stream(self.device)   # filtering of new views
             self.copy_stream = torch.cuda.Stream(self.device)     # host -> device raw counts
             self._tables = _FilterTables(C, window, self.device)
+            # per-view constants of the whole orbit, computed once: the filter records
+            # (slot filled in per call) and a device copy of the view records
+            if self.kind == "cone":
+                self._fv_all = cone_filter_views(self._K_all, R, C, self._tables.n_fft, 0)
+            else:
+                self._fv_all = parallel_filter_views(geom.pixel_u, self.n_total, self._tables.n_fft, 0)
+            self._maps_dev = torch.from_numpy(self._maps_all.view(np.uint8).copy()).to(self.device)
             self._ring = torch.zeros((self.n_total, R, self._pitch), dtype=tdtype, device=self.device)
             self._views_host = np.zeros(self.n_total, dtype=N.VIEW_DTYPE)
             self._views_dev = torch.zeros(self.n_total * N.VIEW_DTYPE.itemsize, dtype=torch.uint8,
@@ -642,19 +658,31 @@ class SliceReconstructor:
 
     # ----------------------------------------------------------- ingest
     def _filter_views(self, idx, slots):
-        R, C = self.geom.rows, self.geom.cols
-        n_fft = self._tables.n_fft
-        if self.kind == "parallel":
-            return parallel_filter_views(self.geom.pixel_u, len(idx), n_fft, slots)
-        K = {k: v[idx] for k, v in self._K_all.items()}
-        return cone_filter_views(K, R, C, n_fft, slots)
+        """mr_filter_view records of geometry views `idx` bound for ring `slots`."""
+        fv = self._fv_all[idx]
+        fv["slot"] = slots
+        return fv
+
+    @staticmethod
+    def _first_of_run(indices):
+        """indices[0] when `indices` are consecutive ascending view numbers, else None."""
+        i0 = int(indices[0])
+        if int(indices[-1]) - i0 == len(indices) - 1 and (len(indices) < 3 or (np.diff(indices) == 1).all()):
+            return i0
+        return None
 
     def _upload_view_records(self, indices, slots):
         """Queue the mr_view records of new slots on the ingest stream (asynchronous)."""
         n0, n1 = slots[0], slots[-1] + 1
-        recs = np.ascontiguousarray(self._maps_all[indices]).view(np.uint8)
+        sz = N.VIEW_DTYPE.itemsize
         with torch.cuda.stream(self.ingest_stream):
-            dst = self._views_dev[n0 * N.VIEW_DTYPE.itemsize:n1 * N.VIEW_DTYPE.itemsize]
+            dst = self._views_dev[n0 * sz:n1 * sz]
+            i0 = self._first_of_run(indices)
+            if i0 is not None:
+                # a run of consecutive views: a device-to-device copy of the orbit's records
+                dst.copy_(self._maps_dev[i0 * sz:(i0 + n1 - n0) * sz], non_blocking=True)
+                return
+            recs = np.ascontiguousarray(self._maps_all[indices]).view(np.uint8)
             # pinned source: the copy is asynchronous and the host does not wait for the
             # ingest kernels queued before it (the caching host allocator keeps the
             # buffer alive until the copy has run)
@@ -666,7 +694,9 @@ class SliceReconstructor:
             n0, n1 = slots[0], slots[-1] + 1
             self._order[n0:n1] = indices
             self._received[indices] = True
-            self._views_host[n0:n1] = self._maps_all[indices]
+            i0 = self._first_of_run(indices)
+            self._views_host[n0:n1] = (self._maps_all[i0:i0 + n1 - n0] if i0 is not None
+                                       else self._maps_all[indices])
             if not uploaded:
                 self._upload_view_records(indices, slots)
             self._chunk_marks = list(marks)
@@ -1062,9 +1092,9 @@ class SliceReconstructor:
             lib = N.load()
             v = ctypes_void
             with torch.cuda.device(self.device), torch.cuda.stream(stream):
-                # one upload for all ranges; launch i reads its own G records
-                g_dev = _struct_tensor(parts, self.device)
-                t_dev = _struct_tensor(tiles, self.device)
+                # one upload for all ranges and the tiles; launch i reads its own G records
+                recs = _struct_tensor(np.concatenate([parts.view(np.uint8), tiles.view(np.uint8)]), self.device)
+                g_ptr, t_ptr = recs.data_ptr(), recs.data_ptr() + parts.nbytes
                 st_ptr = v(self._status.data_ptr())
                 for i, ((a, b), e) in enumerate(zip(zip(bounds[:-1], bounds[1:]), events)):
                     if e is not None:
@@ -1072,14 +1102,13 @@ class SliceReconstructor:
                     tm = self.kernel_timer
                     ev0 = tm.start(stream) if tm is not None else None
                     rc = lib.mr_backproject_staged(self._ring_c, v(self._views_dev.data_ptr()),
-                                                   v(g_dev.data_ptr() + i * G * N.GRID_DTYPE.itemsize),
-                                                   v(t_dev.data_ptr()), len(tiles), v(out.data_ptr()), st_ptr,
+                                                   v(g_ptr + i * G * N.GRID_DTYPE.itemsize),
+                                                   v(t_ptr), len(tiles), v(out.data_ptr()), st_ptr,
                                                    v(stream.cuda_stream))
                     if tm is not None:
                         tm.stop("mr_backproject_staged", ev0, stream)
                     N.check(rc, "mr_backproject_staged")
-                g_dev.record_stream(stream)
-                t_dev.record_stream(stream)
+                recs.record_stream(stream)
             return
         grids["n_views"] = n
         with torch.cuda.device(self.device), torch.cuda.stream(stream):
