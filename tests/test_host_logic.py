@@ -196,3 +196,48 @@ def test_stream_arrival_order_matches_reference():
     np.testing.assert_array_equal(S.arrival_order(5), np.arange(5))
     with pytest.raises(ValueError):
         S.arrival_order(5, "random")
+
+
+def test_cross3_is_numpy_cross_bit_for_bit():
+    rng = np.random.default_rng(3)
+    for _ in range(20000):
+        a = rng.normal(size=3) * 10.0 ** rng.uniform(-4, 4)
+        b = rng.normal(size=3) * 10.0 ** rng.uniform(-4, 4)
+        assert np.cross(a, b).tobytes() == R._cross3(a, b).tobytes()
+    for normal in ((0, 0, 1), (0, 1, 0), (1, 0, 0), (1, 1, 0), (0.3, -0.2, 0.9)):
+        n = np.asarray(normal, float) / np.linalg.norm(normal)
+        z = np.array([0.0, 0.0, 1.0])
+        e1 = np.cross(z, n) if abs(n @ z) < 0.9 else np.cross(n, np.array([0.0, 1.0, 0.0]))
+        e1 /= np.linalg.norm(e1)
+        for x, y in zip(R.plane_basis(normal), (n, e1, np.cross(n, e1))):
+            assert x.tobytes() == y.tobytes()
+
+
+def test_orbit_filter_records_equal_per_call_records():
+    """The reconstructor computes the filter records of the whole orbit once and copies
+    rows per call; they must be the bytes a per-call computation gives."""
+    K = R.cone_constants(G.circular_cone_vectors(120, 440.0, 680.0, 48, 60, 0.3).vectors)
+    full = R.cone_filter_views(K, 48, 60, 128, 0)
+    rng = np.random.default_rng(5)
+    for t in range(40):
+        k = int(rng.integers(1, 120))
+        if t % 2:
+            idx = np.sort(rng.choice(120, k, replace=False))
+        else:
+            a = int(rng.integers(0, 120 - k + 1))
+            idx = np.arange(a, a + k)
+        slots = np.arange(7, 7 + k)
+        want = R.cone_filter_views({key: val[idx] for key, val in K.items()}, 48, 60, 128, slots)
+        got = full[idx]
+        got["slot"] = slots
+        assert got.tobytes() == want.tobytes()
+
+
+def test_first_of_run():
+    f = R.SliceReconstructor._first_of_run
+    assert f(np.arange(5, 9)) == 5
+    assert f(np.array([3])) == 3
+    assert f(np.array([3, 4])) == 3
+    assert f(np.array([4, 3])) is None
+    assert f(np.array([0, 2, 1, 3])) is None          # right span, wrong order
+    assert f(np.array([0, 1, 3])) is None
