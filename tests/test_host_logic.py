@@ -241,3 +241,26 @@ def test_first_of_run():
     assert f(np.array([4, 3])) is None
     assert f(np.array([0, 2, 1, 3])) is None          # right span, wrong order
     assert f(np.array([0, 1, 3])) is None
+
+
+def test_band_ordered_tiles_are_a_permutation_sorted_by_height():
+    rng = np.random.default_rng(9)
+    box = np.array([47.0, 47.0, 37.2])
+    grids = np.zeros(3, dtype=N.GRID_DTYPE)
+    for r in range(3):
+        nrm = rng.normal(size=3)
+        grids[r] = R.plane_grid(box, rng.uniform(-10, 10, 3), nrm / np.linalg.norm(nrm), 200)
+    plain = N.plan_tiles(grids)
+    axis = (0.0, 0.0, 1.0)
+    banded = N.plan_tiles(grids, axis)
+    assert sorted(map(bytes, plain)) == sorted(map(bytes, banded))
+    ti, tj = N.tile_shape()
+    g = grids[banded["grid"]]
+    centre = (g["origin"].astype(np.float64) + (banded["i0"] + (ti - 1) / 2)[:, None] * g["step_i"]
+              + (banded["j0"] + (tj - 1) / 2)[:, None] * g["step_j"])
+    assert np.all(np.diff(centre[:, 2]) <= 1e-9)          # highest first, across the grids
+    assert len(set(banded["grid"][:20])) > 1              # the grids are interleaved
+    # point lists keep the planner's order
+    pts = grids.copy()
+    pts["flags"][1] = N.MR_GRID_POINTS
+    assert N.plan_tiles(pts, axis).tobytes() == N.plan_tiles(pts).tobytes()

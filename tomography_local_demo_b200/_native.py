@@ -146,8 +146,22 @@ def tile_shape():
     return ti.value, tj.value
 
 
-def plan_tiles(grids):
-    """Tiles (numpy TILE_DTYPE array) covering the grids (numpy GRID_DTYPE array)."""
+_TILE_SHAPE = None
+
+
+def plan_tiles(grids, band_axis=None):
+    """Tiles (numpy TILE_DTYPE array) covering the grids (numpy GRID_DTYPE array).
+
+    band_axis: the orbit's rotation axis (the detector's row direction). When given, the
+    tiles of regular grids are ordered by their centre's position along it, highest first,
+    across all grids of the launch. Every view projects tiles at one height onto the same
+    band of detector rows, so the tiles in flight together read one band of the filtered
+    ring instead of footprints spread over the whole detector: their footprint loads then
+    mostly hit L2 (the ring of a scan is larger than L2). The result is the same bit for
+    bit in any order (each tile is summed by one cluster); on a 600-view scan the staged
+    back-projection of three oblique slices ran 3.6 % faster (highest first measured 1-2 %
+    faster than lowest first)."""
+    global _TILE_SHAPE
     grids = np.ascontiguousarray(grids, dtype=GRID_DTYPE)
     lib = load()
     n = _I64()
@@ -155,4 +169,16 @@ def plan_tiles(grids):
     tiles = np.empty(n.value, dtype=TILE_DTYPE)
     check(lib.mr_plan_tiles(grids.ctypes.data, len(grids), tiles.ctypes.data, len(tiles),
                             ctypes.byref(n)), "plan_tiles")
+    if band_axis is not None and len(tiles) > 1 and not (grids["flags"] & MR_GRID_POINTS).any():
+        if _TILE_SHAPE is None:
+            _TILE_SHAPE = tile_shape()
+        a = np.asarray(band_axis, dtype=np.float64)
+        gi = tiles["grid"]
+        o = grids["origin"].astype(np.float64) @ a
+        si = grids["step_i"].astype(np.float64) @ a
+        sj = grids["step_j"].astype(np.float64) @ a
+        sk = grids["step_k"].astype(np.float64) @ a
+        key = (o[gi] + (tiles["i0"] + 0.5 * (_TILE_SHAPE[0] - 1)) * si[gi]
+               + (tiles["j0"] + 0.5 * (_TILE_SHAPE[1] - 1)) * sj[gi] + tiles["k"] * sk[gi])
+        tiles = tiles[np.argsort(-key, kind="stable")]
     return tiles

@@ -269,13 +269,65 @@ def _handoff(stream, *tensors):
             t.record_stream(cur)
 
 
+class _RecordStaging:
+    """Page-locked staging for the small records that go up with every launch: a ring of
+    fixed slots reused in turn, each guarded by the event of its last copy, so the host
+    runs at most `slots` uploads ahead of the GPU. Taking page-locked memory per call
+    instead grows torch's host cache whenever the host runs ahead, and single allocations
+    of that cache took up to 3.5 ms, stalling the launching thread."""
+
+    def __init__(self, slots=32, slot_bytes=128 << 10):
+        self.slot_bytes = slot_bytes
+        self.buf = torch.empty(slots * slot_bytes, dtype=torch.uint8).pin_memory()
+        self.host = self.buf.numpy()
+        self.events = [None] * slots
+        self.next = 0
+        self.lock = threading.Lock()
+
+    def upload(self, raw, device, out=None):
+        """Device copy of the uint8 array `raw` on the current stream (asynchronous), into
+        `out` when given, or None when it does not fit a slot."""
+        n = raw.size
+        if n > self.slot_bytes:
+            return None
+        with self.lock:
+            k = self.next
+            self.next = (k + 1) % len(self.events)
+            if self.events[k] is not None:
+                self.events[k].synchronize()         # the slot's previous copy has run
+            o = k * self.slot_bytes
+            self.host[o:o + n] = raw
+            dst = torch.empty(n, dtype=torch.uint8, device=device) if out is None else out
+            dst.copy_(self.buf[o:o + n], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.current_stream(device))
+            self.events[k] = ev
+        return dst
+
+
+_STAGING = {}
+_STAGING_LOCK = threading.Lock()
+
+
+def _staging(device):
+    """The record staging ring of `device` (created on first use)."""
+    key = torch.device(device).index
+    with _STAGING_LOCK:
+        if key not in _STAGING:
+            _STAGING[key] = _RecordStaging()
+        return _STAGING[key]
+
+
 def _struct_tensor(records, device, asynchronous=False):
     """Device copy of numpy ABI records on the current stream. By default a small pageable
     copy, which the host waits for but which is not queued behind large pinned transfers
     that other streams have in flight; asynchronous=True stages it in page-locked memory
     instead, so the host does not wait (for when no such transfer is in flight)."""
-    raw = np.ascontiguousarray(records).view(np.uint8)
+    raw = np.ascontiguousarray(records).view(np.uint8).reshape(-1)
     if asynchronous:
+        dst = _staging(device).upload(raw, device)
+        if dst is not None:
+            return dst
         return torch.from_numpy(raw.copy()).pin_memory().to(device, non_blocking=True)
     return torch.from_numpy(raw.copy()).to(device, non_blocking=False)
 
@@ -334,7 +386,7 @@ class KernelTimer:
 
 
 def backproject_device(ring, views_dev, grids, out, stream, device, timer=None, kernel="staged",
-                       status=None, wait=None, asynchronous=False):
+                       status=None, wait=None, asynchronous=False, band_axis=None):
     """Back-project numpy GRID_DTYPE records into the device f32 tensor `out`.
 
     kernel="staged": regular grids go through mr_backproject_staged (TMA-staged
@@ -342,7 +394,8 @@ def backproject_device(ring, views_dev, grids, out, stream, device, timer=None, 
     mr_backproject (direct global gathers) - the plain GPU path kept for comparison.
     wait: an event the launch must follow (the filter of the views summed); the grid and
     tile records are uploaded before the stream waits for it (asynchronously from
-    page-locked memory with asynchronous=True)."""
+    page-locked memory with asynchronous=True). band_axis: the orbit's rotation axis, which
+    orders the tiles of regular grids by height (_native.plan_tiles)."""
     grids = np.ascontiguousarray(grids, dtype=N.GRID_DTYPE)
     is_pts = (grids["flags"] & N.MR_GRID_POINTS) != 0
     if kernel == "staged" and is_pts.any() and not is_pts.all():
@@ -351,7 +404,7 @@ def backproject_device(ring, views_dev, grids, out, stream, device, timer=None, 
         wait = None
         grids = grids[~is_pts]
         is_pts = is_pts[~is_pts]
-    tiles = N.plan_tiles(grids)
+    tiles = N.plan_tiles(grids, band_axis)
     if len(tiles) == 0:
         if wait is not None:
             stream.wait_event(wait)
@@ -596,12 +649,18 @@ class SliceReconstructor:
         if isinstance(geom, ParallelGeometry):
             self.kind = "parallel"
             self._kind_code = N.MR_PARALLEL
+            self._band_axis = (0.0, 0.0, 1.0)      # detector rows follow z
             self._maps_all = parallel_view_maps(geom.angles, geom.pixel_u, geom.pixel_v, R, C)
         elif isinstance(geom, ConeVecGeometry):
             self.kind = "cone"
             self._kind_code = N.MR_CONE
             self._K_all = cone_constants(geom.vectors)
             self._maps_all = cone_view_maps(self._K_all, R, C)
+            # the orbit's axis as the mean detector row direction (tile order only)
+            vm = np.asarray(geom.vectors, dtype=np.float64)[:, 9:12]
+            vm = (vm / np.linalg.norm(vm, axis=1, keepdims=True)).mean(0)
+            nrm = float(np.linalg.norm(vm))
+            self._band_axis = tuple(vm / nrm) if nrm > 1e-6 else None
             if geom.angular_range < 2 * np.pi - 1e-3 and verbose and not parker:
                 print("note: short scan (<360 deg) - no Parker weights, expect some artefacts")
         else:
@@ -620,6 +679,7 @@ class SliceReconstructor:
             else:
                 self._fv_all = parallel_filter_views(geom.pixel_u, self.n_total, self._tables.n_fft, 0)
             self._maps_dev = torch.from_numpy(self._maps_all.view(np.uint8).copy()).to(self.device)
+            _staging(self.device)               # page-locked record staging, taken up front
             self._ring = torch.zeros((self.n_total, R, self._pitch), dtype=tdtype, device=self.device)
             self._views_host = np.zeros(self.n_total, dtype=N.VIEW_DTYPE)
             self._views_dev = torch.zeros(self.n_total * N.VIEW_DTYPE.itemsize, dtype=torch.uint8,
@@ -682,11 +742,11 @@ class SliceReconstructor:
                 # a run of consecutive views: a device-to-device copy of the orbit's records
                 dst.copy_(self._maps_dev[i0 * sz:(i0 + n1 - n0) * sz], non_blocking=True)
                 return
-            recs = np.ascontiguousarray(self._maps_all[indices]).view(np.uint8)
-            # pinned source: the copy is asynchronous and the host does not wait for the
-            # ingest kernels queued before it (the caching host allocator keeps the
-            # buffer alive until the copy has run)
-            dst.copy_(torch.from_numpy(recs.copy()).pin_memory(), non_blocking=True)
+            # page-locked staging: the copy is asynchronous and the host does not wait for
+            # the ingest kernels queued before it
+            recs = np.ascontiguousarray(self._maps_all[indices]).view(np.uint8).reshape(-1)
+            if _staging(self.device).upload(recs, self.device, out=dst) is None:
+                dst.copy_(torch.from_numpy(recs.copy()).pin_memory(), non_blocking=True)
 
     def _admit(self, indices, slots, event, uploaded=False, marks=()):
         """Make filtered slots visible to reconstructions (under the state lock)."""
@@ -830,8 +890,7 @@ class SliceReconstructor:
                 # before any chunk is filtered, so a reconstruction may use the first
                 # chunks of this call while the later ones are still on the bus)
                 fv_host = self._filter_views(indices, slots)
-                fv_pinned = torch.from_numpy(np.ascontiguousarray(fv_host).view(np.uint8).copy()).pin_memory()
-                fv = fv_pinned.to(self.device, non_blocking=True)
+                fv = _struct_tensor(fv_host, self.device, asynchronous=True)
                 self._upload_view_records(indices, slots)
                 return fv
 
@@ -1086,7 +1145,7 @@ class SliceReconstructor:
                 sl = slice(i * G, (i + 1) * G)
                 parts["view_begin"][sl], parts["n_views"][sl] = a, b - a
                 parts["accumulate"][sl] = 0 if i == 0 else 1
-            tiles = N.plan_tiles(grids)              # the same tiles for every view range
+            tiles = N.plan_tiles(grids, self._band_axis)     # the same tiles for every view range
             if len(tiles) == 0:
                 return
             lib = N.load()
@@ -1116,7 +1175,7 @@ class SliceReconstructor:
             # the copy engines): the records go up without the host waiting
             backproject_device(self._ring_c, self._views_dev, grids, out, stream, self.device,
                                self.kernel_timer, self.bp_kernel, self._status, wait=event,
-                               asynchronous=not self._chunk_marks)
+                               asynchronous=not self._chunk_marks, band_axis=self._band_axis)
 
     def reconstruct_points_tensor(self, pts, cor_shift=None):
         """Device variant of reconstruct_points: pts (M, 3) -> f32 tensor [M]."""

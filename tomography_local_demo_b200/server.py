@@ -196,7 +196,7 @@ class SliceServer:
             off += int(np.prod(r.shape))
         grids["n_views"] = n_views
         grids["scale"] = np.pi / n_views if n_views else 0.0
-        tiles = N.plan_tiles(grids)
+        tiles = N.plan_tiles(grids, getattr(rec, "_band_axis", None))
         if len(tiles) > self.max_tiles:
             raise MemoryError(f"batch needs {len(tiles)} tiles > {self.max_tiles}")
         st = slot.stream
