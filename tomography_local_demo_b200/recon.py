@@ -732,12 +732,19 @@ class SliceReconstructor:
         return None
 
     def _upload_view_records(self, indices, slots):
-        """Queue the mr_view records of new slots on the ingest stream (asynchronous)."""
+        """Queue the mr_view records of new slots on the ingest stream (asynchronous). This
+        is the only writer of the device table and keeps `_views_host` as its mirror, so
+        slots that already hold the same records - a new scan of the same orbit in the same
+        order after reset() - need no copy. Called under the ingest lock."""
         n0, n1 = slots[0], slots[-1] + 1
         sz = N.VIEW_DTYPE.itemsize
+        i0 = self._first_of_run(indices)
+        new = self._maps_all[i0:i0 + n1 - n0] if i0 is not None else self._maps_all[indices]
+        if new.tobytes() == self._views_host[n0:n1].tobytes():
+            return
+        self._views_host[n0:n1] = new
         with torch.cuda.stream(self.ingest_stream):
             dst = self._views_dev[n0 * sz:n1 * sz]
-            i0 = self._first_of_run(indices)
             if i0 is not None:
                 # a run of consecutive views: a device-to-device copy of the orbit's records
                 dst.copy_(self._maps_dev[i0 * sz:(i0 + n1 - n0) * sz], non_blocking=True)
@@ -754,9 +761,6 @@ class SliceReconstructor:
             n0, n1 = slots[0], slots[-1] + 1
             self._order[n0:n1] = indices
             self._received[indices] = True
-            i0 = self._first_of_run(indices)
-            self._views_host[n0:n1] = (self._maps_all[i0:i0 + n1 - n0] if i0 is not None
-                                       else self._maps_all[indices])
             if not uploaded:
                 self._upload_view_records(indices, slots)
             self._chunk_marks = list(marks)
@@ -890,7 +894,14 @@ class SliceReconstructor:
                 # before any chunk is filtered, so a reconstruction may use the first
                 # chunks of this call while the later ones are still on the bus)
                 fv_host = self._filter_views(indices, slots)
-                fv = _struct_tensor(fv_host, self.device, asynchronous=True)
+                # the filter records go up on the copy stream: unlike the view records they
+                # do not wait for the reconstructions that still read the ring
+                with torch.cuda.stream(self.copy_stream):
+                    fv = _struct_tensor(fv_host, self.device, asynchronous=True)
+                    fv_ready = torch.cuda.Event()
+                    fv_ready.record(self.copy_stream)
+                self.ingest_stream.wait_event(fv_ready)
+                fv.record_stream(self.ingest_stream)
                 self._upload_view_records(indices, slots)
                 return fv
 
