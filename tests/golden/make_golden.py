@@ -174,7 +174,52 @@ def main(ref_root):
     vol[vol < 0.05] = 0
     save("misc.npz", otsu_vol=vol, otsu=M.otsu_threshold(vol), **d)
     loader_fixtures(FX, H5, save)
+    net_fixtures(save)
     print("golden fixtures written to", HERE, "from minirecast", minirecast.__version__)
+
+
+class _Recorder:
+    """A connection stand-in that keeps every payload passed to send_bytes."""
+
+    def __init__(self):
+        self.payloads = []
+
+    def send_bytes(self, b):
+        self.payloads.append(bytes(b))
+
+
+def net_messages():
+    """(header, array) pairs covering the reference's message kinds."""
+    rng = np.random.default_rng(11)
+    return [({"cmd": "hello", "role": "adapter"}, None),
+            ({"cmd": "projections", "indices": [3, 1, 2]}, rng.normal(size=(4, 3, 5)).astype(np.float32)),
+            ({"version": 7}, rng.normal(size=(6, 6)).astype(np.float32)),
+            ({"origin": [0.5, -1.0, 2.0], "spacing": 0.25}, rng.gamma(2.0, 1.0, (2, 3, 4)).astype(np.float32)),
+            ({"cmd": "raw", "note": "u16"}, rng.integers(0, 65535, (2, 3, 4)).astype(np.uint16)),
+            ({"cmd": "slice", "origin": [0.0, 0.0, 0.0], "normal": [0.0, 0.0, 1.0], "n": 64, "zoom": 1.0,
+              "center": None}, None)]
+
+
+def net_fixtures(save):
+    """Payloads of the reference's net.send for the messages of net_messages(), and its
+    geometry messages for a cone and a parallel scan."""
+    from minirecast import net as NET, geometry as G
+    out = {}
+    for i, (h, arr) in enumerate(net_messages()):
+        rec = _Recorder()
+        NET.send(rec, h, arr)
+        for j, b in enumerate(rec.payloads):
+            out[f"m{i}_p{j}"] = np.frombuffer(b, dtype=np.uint8)
+        out[f"m{i}_count"] = np.array(len(rec.payloads))
+    cone = G.circular_cone_vectors(12, 300.0, 600.0, 8, 10, 1.5, det_shift_u=0.7)
+    par = G.ParallelGeometry(np.linspace(0, np.pi, 9, endpoint=False), 6, 7, 0.5, 0.25)
+    for tag, geom in (("cone", cone), ("par", par)):
+        h, arr = NET.geometry_message(geom)
+        rec = _Recorder()
+        NET.send(rec, h, arr)
+        out[f"geom_{tag}_p0"] = np.frombuffer(rec.payloads[0], dtype=np.uint8)
+        out[f"geom_{tag}_p1"] = np.frombuffer(rec.payloads[1], dtype=np.uint8)
+    save("net_frames.npz", **out)
 
 
 def loader_fixtures(FX, H5, save):
@@ -199,4 +244,11 @@ def loader_fixtures(FX, H5, save):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    root = args[0] if args else "/root/reference"
+    if "--net-only" in sys.argv:                 # only net_frames.npz
+        os.environ.setdefault("NUMBA_CACHE_DIR", tempfile.mkdtemp(prefix="numba_cache_"))
+        sys.path.insert(0, root)
+        net_fixtures(lambda name, **kw: np.savez_compressed(os.path.join(HERE, name), **kw))
+    else:
+        main(root)

@@ -766,7 +766,7 @@ class SliceReconstructor:
             self._chunk_marks = list(marks)
             event.record(self.ingest_stream)
             self._ingest_event = event
-            self.n = n1
+            self.n = int(n1)
             self.version += 1
             return self.n
 
