@@ -120,6 +120,14 @@ def test_framing_over_a_pipe_reuses_buffers_and_refuses_non_numbers():
     a.send_bytes(b"\x00" * 12)                        # 3 floats where 4 were announced
     with pytest.raises(ValueError):
         net.recv(b, pool)
+    for shape in ([-1, 4], [1 << 20, 1 << 20]):       # negative / beyond the payload limit
+        a.send_bytes(('{"_array": {"dtype": "<f4", "shape": %s}}' % shape).encode())
+        with pytest.raises(ValueError):
+            net.recv(b, pool)
+    small = net.PinnedFrames(pinned=False, keep_bytes=8)
+    small.release(small.take(64))                     # above keep_bytes: not kept
+    small.release(small.take(8))
+    assert [t.numel() for t, _ in small._free] == [8]
 
 
 def test_bf16_replies_round_to_nearest_even():

@@ -35,6 +35,7 @@ from .recon import SliceReconstructor, plane_size_for_box, slice_points
 from .server import SliceServer
 
 DEFAULT_PORT = 5558
+MAX_ARRAY_BYTES = 1 << 36           # largest array payload accepted (64 GiB)
 
 
 def authkey():
@@ -84,6 +85,8 @@ def recv(conn, frames=None):
         return header, None
     dtype, shape = spec
     nbytes = int(np.prod(shape, dtype=np.int64)) * dtype.itemsize
+    if any(d < 0 for d in shape) or nbytes > MAX_ARRAY_BYTES:
+        raise ValueError(f"refusing an array of shape {shape} ({nbytes} bytes)")
     if frames is None or not dtype.isnative:
         data = conn.recv_bytes()
         if len(data) != nbytes:
@@ -109,11 +112,13 @@ class PinnedFrames:
     """Reusable page-locked receive buffers. `take(n)` returns a uint8 tensor of at least
     n bytes whose previous contents are no longer read by any queued device copy;
     `release(buf, streams)` returns it to the pool once the copies queued on `streams`
-    so far have run. Buffers grow to the largest payload seen; `pinned=False` gives
-    ordinary host memory (no CUDA needed)."""
+    so far have run. Buffers grow to the largest payload seen; one larger than `keep_bytes`
+    is not kept (torch's host cache holds it until the copies that read it have run).
+    `pinned=False` gives ordinary host memory (no CUDA needed)."""
 
-    def __init__(self, pinned=True):
+    def __init__(self, pinned=True, keep_bytes=1 << 30):
         self.pinned = pinned and torch.cuda.is_available()
+        self.keep_bytes = int(keep_bytes)
         self._free = []                 # [(uint8 buffer, [events])]
         self._lent = {}                 # data pointer of a lent view -> its uint8 buffer
         self._lock = threading.Lock()
@@ -142,6 +147,8 @@ class PinnedFrames:
         """Return a buffer, or an array that recv() lent from one, to the pool."""
         with self._lock:
             base = self._lent.pop(buf.data_ptr(), buf)
+        if base.numel() > self.keep_bytes:
+            return
         events = []
         for st in streams:
             ev = torch.cuda.Event()
