@@ -605,6 +605,12 @@ def run_case(args):
     surface     model.marching_cubes of a 640^3 float32 volume (a noisy ball of radius 250)
     correct     the loaders' correction + crop (mr_correct_u16) of 120 views 1944 x 1536
     ingest-full the fused FFT ingest of 1200 raw views 1944 x 1536 into a bf16 ring
+    parker      the ingest of a 600-view short scan (pi + fan angle) of 486 x 384 raw views
+                with Parker weights (correction, weighting, tensor-core filter), beside
+                the same ingest without them
+    wire        a scan through the wire-compatible service on 127.0.0.1: per step, reset,
+                600 raw views of 486 x 384 pushed in messages of 50 views, then three
+                512^2 slices back in one BF16 reply (host wall clock)
     Prints one JSON line: the case's own throughput and its HBM figure."""
     import torch
     from tomography_local_demo_b200 import SliceReconstructor, circular_cone_vectors
@@ -638,6 +644,38 @@ def run_case(args):
                                        v(gain.data_ptr()), C0, N.MR_CORRECT_FLEXRAY, v(out.data_ptr()), k * C0, C0,
                                        v(torch.cuda.current_stream().cuda_stream)), "mr_correct_u16")
         units, unit, nbytes = k, "views/s", k * R0 * C0 * (2 + 4)
+    elif args.case == "parker":
+        V, R0, C0 = args.case_views or 600, 384, 486
+        w = WORKLOAD
+        fan = float(np.arctan(0.5 * C0 * w["pixel"] / w["sdd"]))
+        # the last view sits one step short of the range: cover 180 deg + fan angle with it
+        geom = circular_cone_vectors(V, w["sod"], w["sdd"], R0, C0, w["pixel"],
+                                     angular_range=(np.pi + 2 * fan) * V / (V - 1) * 1.001)
+        raw = torch.randint(30000, 50000, (V, R0, C0), generator=gen, device=dev, dtype=torch.int32).to(torch.int16)
+        recs = {}
+        for pk in (True, False):
+            recs[pk] = SliceReconstructor(None, geom, store="bf16", verbose=False, filter="tc", parker=pk)
+            recs[pk].set_flat_dark(np.full((2, R0, C0), 50000, np.uint16), np.full((2, R0, C0), 100, np.uint16))
+        idx = np.arange(V)
+
+        def ingest(rec):
+            rec.reset()
+            rec.add_raw_projections(idx, raw)
+            torch.cuda.current_stream().wait_stream(rec.ingest_stream)
+        step = lambda: ingest(recs[True])                          # noqa: E731
+        units, unit, nbytes = V, "views/s", V * R0 * C0 * (2 + 2)
+        for _ in range(args.warmup):
+            ingest(recs[False])
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(args.steps):
+            ingest(recs[False])
+        a1.record()
+        torch.cuda.synchronize()
+        extra = {"without_parker_ms": a0.elapsed_time(a1) / args.steps}
+    elif args.case == "wire":
+        return run_wire_case(args)
     else:
         V, R0, C0 = args.case_views or 1200, 1536, 1944
         geom = circular_cone_vectors(V, 440.0, 680.0, R0, C0, 0.0748)
@@ -667,10 +705,54 @@ def run_case(args):
     except (OSError, ValueError, KeyError):
         peak, source = 6650.0, "fallback"
     gbs = nbytes / ms / 1e6
-    return {"case": args.case, "metric": unit.split("/")[0] + " per second", "value": units / ms * 1e3,
+    line = {"case": args.case, "metric": unit.split("/")[0] + " per second", "value": units / ms * 1e3,
             "unit": unit, "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
             "hbm": {"algorithmic_bytes": nbytes, "achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak,
                     "peak_source": source}}
+    if args.case == "parker":
+        line.update(extra)
+    return line
+
+
+def run_wire_case(args):
+    """The `wire` case of run_case: host wall clock per step through net.Server."""
+    import threading
+    import torch
+    from tomography_local_demo_b200 import net
+    dev = torch.device("cuda", 0)
+    geom, raw_dev, flats, darks = make_scan(dev)
+    raw = raw_dev.cpu().numpy().view(np.uint16)
+    reqs = slice_requests(geom.volume_box())
+    srv = net.Server(port=0, verbose=False, store="bf16", filter="tc", budget_bytes=1 << 30)
+    address = srv.listen()
+    threading.Thread(target=srv.serve_forever, daemon=True).start()
+    sink = net.RemoteSink(address, geom)
+    sink.set_flat_dark(as_u16(flats), as_u16(darks))
+    view = net.RemoteReconstructor(address, encoding="bf16")
+    V, group = WORKLOAD["views"], 50
+
+    def step():
+        sink.reset()
+        for g0 in range(0, V, group):
+            idx = np.arange(g0, min(V, g0 + group))
+            sink.add_raw_projections(idx, raw[idx])
+        return view.reconstruct_planes(reqs)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    ms = (time.perf_counter() - t0) / args.steps * 1e3
+    for c in (view, sink):
+        c.close()
+    srv.close()
+    raw_bytes = raw.nbytes
+    reply = sum(r["n"] ** 2 for r in reqs) * 2
+    return {"case": "wire", "metric": "views per second", "value": V / ms * 1e3, "unit": "views/s",
+            "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup, "clock": "host wall clock",
+            "bytes_per_step": {"requests": raw_bytes, "replies": reply},
+            "wire_gbs": (raw_bytes + reply) / ms / 1e6}
 
 
 def main():
@@ -684,7 +766,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the live-scan serving simulation")
     ap.add_argument("--filter", choices=("fft", "tc", "tc-bf16"), default="tc",
                     help="row filter: shared-memory FFT or tensor-core Toeplitz GEMM (split FP16 / BF16)")
-    ap.add_argument("--case", choices=("otsu", "surface", "correct", "ingest-full"), default=None,
+    ap.add_argument("--case", choices=("otsu", "surface", "correct", "ingest-full", "parker", "wire"), default=None,
                     help="time one other kernel family alone instead of the headline step")
     ap.add_argument("--case-views", type=int, default=0, help="views of the correct / ingest-full case")
     args = ap.parse_args()

@@ -97,9 +97,15 @@ def test_raw_projections_through_the_fused_ingest(server):
         assert n_remote == local.add_raw_projections(part, torch.from_numpy(raw[part].view(np.int16)).cuda())
     view = net.RemoteReconstructor(address)
     assert view.n == 40
-    for r in REQS:
+    want = [_local(local, r).astype(np.float64) for r in REQS]
+    for r, w in zip(REQS, want):
         img, _ = view.reconstruct_plane(r["origin"], r["normal"], n=r["n"], zoom=r["zoom"])
-        np.testing.assert_array_equal(img, _local(local, r).astype(np.float64))
+        np.testing.assert_array_equal(img, w)
+    sink.reset()                                            # a new scan, same geometry
+    assert view.n == 0
+    sink.add_raw_projections(order, raw[order])
+    for got, w in zip(view.reconstruct_planes(REQS), want):
+        np.testing.assert_array_equal(got, w)
     view.close()
     sink.close()
 

@@ -49,3 +49,18 @@ def test_errors():
         parker_weights(circular_cone_vectors(100, 300.0, 600.0, 8, 16, 3.0).vectors, 16)
     with pytest.raises(ValueError, match="fan angle"):
         parker_weights(_short(extra=0.05), 64)
+
+
+def test_plateau_views_form_one_run_in_the_middle():
+    """The raw ingest folds the weight of views that are at the plateau in every column into
+    the filter's output scale: those views are one run in the middle of the short scan,
+    with every weight exactly the plateau value, and the rest ramp below it."""
+    fan = np.arctan(0.5 * 486 * 0.299 / 680.0)
+    V = 600
+    g = circular_cone_vectors(V, 440.0, 680.0, 384, 486, 0.299, angular_range=(np.pi + 2 * fan) * V / (V - 1) * 1.001)
+    w = parker_weights(g.vectors, 486)
+    flat = np.all(w == w.max(), axis=1)
+    run = np.flatnonzero(flat)
+    assert len(run) > 0.6 * V and np.all(np.diff(run) == 1)
+    assert run[0] > 0 and run[-1] < V - 1
+    assert np.all(w[~flat].min(axis=1) < w.max())

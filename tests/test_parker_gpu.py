@@ -66,8 +66,20 @@ def test_parker_raw_counts_and_input_untouched(cuda):
     keep = blk.clone()
     b.add_projections(np.arange(short.n_angles), blk)
     assert torch.equal(blk, keep)                                    # the caller's block is not weighted
+    # the same counts in bit-reversed arrival order, in three calls: plateau views go through
+    # the fused ingest, the ramped ones through correction + weights + filter, in any mix
+    from tomography_local_demo_b200.stream import arrival_order
+    c = SliceReconstructor(None, short, parker=True, verbose=False, filter="tc")
+    c.set_flat_dark(flat, dark)
+    order = arrival_order(short.n_angles, "interleaved")
+    for part in np.array_split(order, 3):
+        c.add_raw_projections(part, torch.from_numpy(raw[part].view(np.int16)).cuda())
+    assert c.n == short.n_angles
+    assert 0 < c._parker_flat.sum() < short.n_angles
     for o, nrm in PLANES:
-        assert rel_l2(a.reconstruct_plane(o, nrm, n=48)[0], b.reconstruct_plane(o, nrm, n=48)[0]) < 1e-5
+        want = b.reconstruct_plane(o, nrm, n=48)[0]
+        assert rel_l2(a.reconstruct_plane(o, nrm, n=48)[0], want) < 1e-5
+        assert rel_l2(c.reconstruct_plane(o, nrm, n=48)[0], want) < 5e-5
 
 
 def test_parker_option_errors(cuda):

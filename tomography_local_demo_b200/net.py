@@ -18,7 +18,8 @@ Beyond the reference:
 * "slice" and "slices" take "encoding": "bf16": the reply carries each FP32 value rounded
   to nearest-even BF16 as uint16 (half the bytes; the reference's `recv` accepts it as an
   integer array) and says so in the header; `decode_image` widens it back;
-* "slices" answers several slice requests with one array;
+* "slices" answers several slice requests with one array; "reset" starts a new scan with
+  the same geometry;
 * slices and previews are answered by the continuously batched `SliceServer`.
 """
 import json
@@ -327,6 +328,10 @@ class Server:
             rec.set_flat_dark(a[0], a[1], bin=int(h.get("bin", 1)), flip_rows=bool(h.get("flip_rows", False)),
                               mode=h.get("mode", "flexray"))
             send(conn, {"ok": True})
+        elif cmd == "reset":
+            rec, _ = self._current()
+            rec.reset()
+            send(conn, {"ok": True})
         elif cmd == "end":
             rec, _ = self._current()
             self.log(f"[server] adapter finished ({rec.n} projections)")
@@ -502,6 +507,10 @@ class RemoteSink:
         h, _ = self._c.call({"cmd": "raw_projections", "indices": [int(i) for i in np.asarray(indices).ravel()]},
                             np.asarray(raw, dtype=np.uint16))
         return h.get("n")
+
+    def reset(self):
+        """A new scan with the same geometry (the server forgets the received views)."""
+        self._c.call({"cmd": "reset"})
 
     def end(self):
         self._c.call({"cmd": "end"})

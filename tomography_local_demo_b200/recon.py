@@ -222,6 +222,13 @@ def parallel_filter_views(pixel_u, k, n_fft, slots, out_scale=1.0):
 # --------------------------------------------------------------------------
 # Device helpers
 # --------------------------------------------------------------------------
+# |-log(max(t, 1e-3))| of corrected raw counts stays below 11.1 when t <= 65535 (FleX-ray
+# gain 1 / max(F - D, 1)); the tensor-core input scale it gives (1024, as in the fused raw
+# ingest) keeps any |x| < 64 inside FP16's range, which covers the HDF5 gain
+# 1 / max(F - D, 1e-6) too (|x| < 25)
+RAW_LINE_BOUND = 11.1
+
+
 def _device(device=None):
     if not torch.cuda.is_available():
         raise RuntimeError("a CUDA device is required: this library has no CPU path")
@@ -332,15 +339,21 @@ def _struct_tensor(records, device, asynchronous=False):
     return torch.from_numpy(raw.copy()).to(device, non_blocking=False)
 
 
-def filter_block_device(block, s_view, s_row, k, fviews_dev, tables, ring, stream, method="fft", status=None):
+def filter_block_device(block, s_view, s_row, k, fviews_dev, tables, ring, stream, method="fft", status=None,
+                        x_bound=None):
     """Filter k views of a device f32 block into ring slots: mr_filter_f32 (FFT) or
-    mr_filter_f32_tc (tensor-core Toeplitz GEMM, split FP16 "tc" or split BF16 "tc-bf16")."""
+    mr_filter_f32_tc (tensor-core Toeplitz GEMM, split FP16 "tc" or split BF16 "tc-bf16").
+    x_bound: a known bound on |block| (the tensor-core input scale is then set from it,
+    without reading the block back to the host)."""
     lib = N.load()
     if method in ("tc", "tc-bf16"):
         fmt = N.MR_BF16 if method == "tc-bf16" else N.MR_F16
         img, t_scale = tables.tc_image(fmt)
         # power of two with max |x| * x_scale in [2^13, 2^14) (FP16 range for the hi part)
-        m = float(block.abs().amax()) if block.numel() else 0.0
+        if x_bound is not None:
+            m = float(x_bound)
+        else:
+            m = float(block.abs().amax()) if block.numel() else 0.0
         x_scale = 2.0 ** int(np.clip(14 - np.frexp(m)[1], -100, 100)) if m > 0 and np.isfinite(m) else 1.0
         st = lib.mr_filter_f32_tc(ctypes_void(block.data_ptr()), s_view, s_row, k,
                                   ctypes_void(fviews_dev.data_ptr()), ctypes_void(img.data_ptr()), fmt, t_scale,
@@ -690,7 +703,11 @@ class SliceReconstructor:
             if self.kind != "cone":
                 raise ValueError("Parker weights apply to cone-beam orbits")
             with torch.cuda.device(self.device):
-                self._parker = torch.from_numpy(parker_weights(geom.vectors, C).astype(np.float32)).to(self.device)
+                pw = parker_weights(geom.vectors, C)
+                self._parker = torch.from_numpy(pw.astype(np.float32)).to(self.device)
+            # views weighted by the plateau value in every column (most of the orbit)
+            self._parker_plateau = float(pw.max())
+            self._parker_flat = np.all(pw == pw.max(), axis=1)
         self._proj = None               # unfiltered line integrals [n_total, R, pitch] (keep_projections)
         if keep_projections:
             with torch.cuda.device(self.device):
@@ -772,6 +789,10 @@ class SliceReconstructor:
 
     def add_projections(self, indices, block):
         """Add projections (geometry indices `indices`, data [rows, k, cols] float32)."""
+        return self._add_block(indices, block)
+
+    def _add_block(self, indices, block, x_bound=None):
+        """add_projections; x_bound: a known bound on |block| (see filter_block_device)."""
         indices = np.asarray(indices, dtype=np.int64).ravel()
         is_tensor = isinstance(block, torch.Tensor)
         if not is_tensor:
@@ -797,13 +818,16 @@ class SliceReconstructor:
                     self._proj[n0:n0 + k, :, :C] = torch.as_strided(x, (k, R, C), (s_view, s_row, 1))
                 if self._parker is not None:
                     # short-scan weights on a copy (x may be the caller's own tensor)
-                    w = self._parker[torch.from_numpy(indices).to(self.device)]          # [k, C]
+                    idx_dev = _struct_tensor(indices, self.device, asynchronous=True).view(torch.int64)
+                    w = self._parker.index_select(0, idx_dev)                            # [k, C]
                     xw = torch.empty((k, R, C), dtype=torch.float32, device=self.device)
                     torch.mul(torch.as_strided(x, (k, R, C), (s_view, s_row, 1)), w[:, None, :], out=xw)
                     x, s_view, s_row = xw, R * C, C
                 fv = _struct_tensor(self._filter_views(indices, slots), self.device)
                 filter_block_device(x, s_view, s_row, k, fv, self._tables, self._ring_c,
-                                    self.ingest_stream, self.filter_method, self._status)
+                                    self.ingest_stream, self.filter_method, self._status,
+                                    None if x_bound is None else x_bound * (self._parker_plateau
+                                                                            if self._parker is not None else 1.0))
                 ev = torch.cuda.Event()
             return self._admit(indices, slots, ev)
 
@@ -871,9 +895,34 @@ class SliceReconstructor:
             raise ValueError(f"raw frames {tuple(raw.shape[1:])} are smaller than "
                              f"{R * b} x {C * b}")
         if self._parker is not None:
-            # short scan: the Parker weights go between the correction and the filter, so
-            # the counts are corrected on their own (mr_correct_u16) and filtered as a block
-            return self.add_projections(indices, self._correct_raw(raw))
+            return self._add_raw_parker(indices, raw)
+        return self._add_raw_fused(indices, raw)
+
+    def _add_raw_parker(self, indices, raw):
+        """Short scan: a view whose Parker weight is the plateau value for every column
+        (the middle of the orbit) goes through the fused ingest with that value folded into
+        the filter's output scale (the filter is linear); the others are corrected on their
+        own (mr_correct_u16), weighted per column and filtered as a block."""
+        const = self._parker_flat[indices]
+        if const.all():
+            return self._add_raw_fused(indices, raw, self._parker_plateau)
+        if not const.any():
+            return self._add_block(indices, self._correct_raw(raw), RAW_LINE_BOUND)
+        flat, ramp = np.flatnonzero(const), np.flatnonzero(~const)
+        self._add_raw_fused(indices[flat], self._views_of(raw, flat), self._parker_plateau)
+        return self._add_block(indices[ramp], self._correct_raw(self._views_of(raw, ramp)), RAW_LINE_BOUND)
+
+    @staticmethod
+    def _views_of(raw, sel):
+        """raw[sel] for raw counts [k, R0, C0] (a view when sel is a run)."""
+        if len(sel) and int(sel[-1]) - int(sel[0]) == len(sel) - 1:
+            return raw[int(sel[0]):int(sel[-1]) + 1]
+        if isinstance(raw, torch.Tensor):
+            return raw[torch.from_numpy(sel).to(raw.device)]
+        return np.asarray(raw)[sel]
+
+    def _add_raw_fused(self, indices, raw, out_scale=1.0):
+        """The fused ingest of add_raw_projections; out_scale multiplies the filtered views."""
         with self._ingest_lock:
             keep = ~self._received[indices]
             if not keep.all():
@@ -894,6 +943,8 @@ class SliceReconstructor:
                 # before any chunk is filtered, so a reconstruction may use the first
                 # chunks of this call while the later ones are still on the bus)
                 fv_host = self._filter_views(indices, slots)
+                if out_scale != 1.0:
+                    fv_host["out_scale"] *= out_scale
                 # the filter records go up on the copy stream: unlike the view records they
                 # do not wait for the reconstructions that still read the ring
                 with torch.cuda.stream(self.copy_stream):
