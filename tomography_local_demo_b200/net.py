@@ -10,9 +10,11 @@ Connections are `multiprocessing.connection` ones, authenticated (HMAC) with the
 key in $MINIRECAST_KEY.
 
 Beyond the reference:
-* receive side: array payloads are read with `recv_bytes_into` straight into page-locked
-  buffers of a reused pool (`PinnedFrames`) and handed to the reconstructor as pinned
-  tensors, so projections go host -> device with no intermediate host copy;
+* receive side: array payloads are read from the connection's descriptor straight into
+  page-locked buffers of a reused pool (`PinnedFrames`) and handed to the reconstructor as
+  pinned tensors, so projections go socket -> page-locked memory -> device with no
+  intermediate host copy (the standard `recv_bytes` / `recv_bytes_into` read into a
+  BytesIO and copy);
 * "raw_projections" (uint16 counts [k, R0, C0] through the fused ingest) and "flat_dark"
   (`set_flat_dark`, flat and dark stacked as [2, n, R0, C0]) commands;
 * "slice" and "slices" take "encoding": "bf16": the reply carries each FP32 value rounded
@@ -24,9 +26,10 @@ Beyond the reference:
 """
 import json
 import os
+import struct
 import threading
 import time
-from multiprocessing.connection import Client, Listener
+from multiprocessing.connection import Client, Connection, Listener
 
 import numpy as np
 import torch
@@ -94,11 +97,43 @@ def recv(conn, frames=None):
             raise ValueError(f"array message of {len(data)} bytes, header announced {nbytes}")
         return header, np.frombuffer(data, dtype=dtype).reshape(shape)
     buf = frames.take(max(nbytes, 1))
-    got = conn.recv_bytes_into(memoryview(buf.numpy()))
+    got = _recv_bytes_into(conn, memoryview(buf.numpy()))
     if got != nbytes:
         frames.release(buf)
         raise ValueError(f"array message of {got} bytes, header announced {nbytes}")
     return header, frames.lend(buf, buf[:nbytes].view(_TORCH_DTYPE[dtype]).view(shape))
+
+
+def _read_exact(fd, view):
+    """Fill `view` from file descriptor `fd` (EOFError if the peer closes first)."""
+    got = 0
+    while got < len(view):
+        n = os.readv(fd, [view[got:]])
+        if n == 0:
+            raise EOFError("connection closed inside a message")
+        got += n
+
+
+def _recv_bytes_into(conn, view):
+    """conn.recv_bytes_into(view) without the intermediate copy: on a POSIX socket or pipe
+    Connection the message's length prefix (4 bytes big-endian, or -1 then 8 bytes for
+    messages over 2 GiB - multiprocessing.connection's framing) is read first and the
+    payload is read from the descriptor straight into `view`. Other connections use
+    recv_bytes_into, which reads the message into a BytesIO and copies it."""
+    if os.name != "posix" or not isinstance(conn, Connection):
+        return conn.recv_bytes_into(view)
+    fd = conn.fileno()
+    head = bytearray(4)
+    _read_exact(fd, memoryview(head))
+    size = struct.unpack("!i", head)[0]
+    if size == -1:
+        head = bytearray(8)
+        _read_exact(fd, memoryview(head))
+        size = struct.unpack("!Q", head)[0]
+    if size > len(view):
+        raise ValueError(f"array message of {size} bytes does not fit its {len(view)}-byte buffer")
+    _read_exact(fd, view[:size])
+    return size
 
 
 _TORCH_DTYPE = {np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64,
