@@ -49,8 +49,6 @@ constexpr int A_TILE_BYTES = TILE_M * 128;      // 128 rows x 64 values (16 KB)
 constexpr int STAGES = 2;
 constexpr int STAGE_BYTES = 2 * A_TILE_BYTES;   // hi + lo
 constexpr unsigned long long WAIT_NS = 2000000000ull;
-constexpr int EPI_ROW_BYTES = 80;
-constexpr int EPI_STAGE_BYTES = 32 * EPI_ROW_BYTES;
 
 struct RowInfo {                                // one GEMM row (detector row of a view)
     const void* src;                            // first input element of the row
@@ -291,11 +289,6 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
     uint64_t* drain = tfull + 2;                // every issued MMA has completed
     volatile int* abort_flag = reinterpret_cast<volatile int*>(drain + 1);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1) + 1;
-    // epilogue staging, per epilogue warp: 32 rows x 80 bytes (64 bytes of values + 16 of
-    // padding: conflict-free both when a lane writes its row and when 8 rows are read out
-    // for coalesced global stores) and the 32 rows' destinations
-    unsigned char* epi_stage = reinterpret_cast<unsigned char*>(drain + 2);
-    unsigned char** epi_rowp = reinterpret_cast<unsigned char**>(epi_stage + EPI_WARPS * EPI_STAGE_BYTES);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -605,11 +598,6 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
             const int nch = (A.pitch + 31) / 32;
             const int nld = (NCOL / 32 < nch) ? NCOL / 32 : nch;         // chunks inside the accumulator
             const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
-            unsigned char* stg = epi_stage + q * EPI_STAGE_BYTES;
-            unsigned char** rowp = epi_rowp + q * 32;
-            rowp[lane] = live ? out : nullptr;
-            // lane -> (row, 16-byte segment) of the read-out: 8 rows per store instruction
-            const int rd_row = lane >> 2, rd_seg = lane & 3;
             for (int ch = 0; ch < nch; ++ch) {
                 float vv[32];
                 if (ch < nld) {                                     // warp-uniform
@@ -620,17 +608,20 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                 }
 #pragma unroll
                 for (int e = 0; e < 32; ++e) vv[e] = (32 * ch + e < A.cols) ? vv[e] * scale : 0.f;
-                // one pass of 32 values (16-bit ring) or two of 16 (FP32): each lane writes its
-                // row's 64 bytes into the staging tile, then the warp stores 8 rows at a time
-                const int passes = A.dtype == MR_F32 ? 2 : 1;
-                for (int h = 0; h < passes; ++h) {
-                    uint4* my = reinterpret_cast<uint4*>(stg + lane * EPI_ROW_BYTES);
+                // each lane stores its own row (view) as 16-byte segments: the L2 merges the
+                // partial sectors, and the warp spends no shared-memory round trip on a
+                // transpose (a staged transpose into coalesced rows measured 6 % slower)
+                if (live) {
+                    const int esz = A.dtype == MR_F32 ? 4 : 2;
+                    const int per = 16 / esz;
                     if (A.dtype == MR_F32) {
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int e = 16 * h + 4 * j;
-                            my[j] = make_uint4(__float_as_uint(vv[e]), __float_as_uint(vv[e + 1]),
-                                               __float_as_uint(vv[e + 2]), __float_as_uint(vv[e + 3]));
+                        for (int j = 0; j < 8; ++j) {
+                            const int col = 32 * ch + 4 * j;
+                            if (col + per <= A.pitch)
+                                *reinterpret_cast<uint4*>(out + col * esz) =
+                                    make_uint4(__float_as_uint(vv[4 * j]), __float_as_uint(vv[4 * j + 1]),
+                                               __float_as_uint(vv[4 * j + 2]), __float_as_uint(vv[4 * j + 3]));
                         }
                     } else {
                         uint32_t w[16];
@@ -645,21 +636,13 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                             }
                         }
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) my[j] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
+                        for (int j = 0; j < 4; ++j) {
+                            const int col = 32 * ch + 8 * j;
+                            if (col + per <= A.pitch)
+                                *reinterpret_cast<uint4*>(out + col * esz) =
+                                    make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
+                        }
                     }
-                    __syncwarp();
-                    const int esz = A.dtype == MR_F32 ? 4 : 2;
-                    const int col = 32 * ch + (A.dtype == MR_F32 ? 16 * h + 4 * rd_seg : 8 * rd_seg);
-                    const int per = 16 / esz;                       // elements per 16-byte segment
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int row = 8 * k + rd_row;
-                        unsigned char* dst = rowp[row];
-                        if (dst != nullptr && col + per <= A.pitch)
-                            *reinterpret_cast<uint4*>(dst + col * esz) =
-                                *reinterpret_cast<const uint4*>(stg + row * EPI_ROW_BYTES + 16 * rd_seg);
-                    }
-                    __syncwarp();
                 }
             }
             fence_before();
@@ -677,7 +660,7 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
 
 inline size_t smem_bytes(int kb) {
     return 1024 + (size_t)(2 * kb - 1 + 3) * BLOCK_BYTES + (size_t)STAGES * STAGE_BYTES + TILE_M * sizeof(RowInfo) +
-           (2 * STAGES + 3) * sizeof(uint64_t) + 16 + EPI_WARPS * (EPI_STAGE_BYTES + 32 * sizeof(void*));
+           (2 * STAGES + 3) * sizeof(uint64_t) + 16;
 }
 
 template <bool RAW>
