@@ -719,6 +719,7 @@ class SliceReconstructor:
         self._raw_dev = None            # device staging of host raw counts (grows on demand)
         self._raw_pinned = []           # pinned staging of pageable raw counts, one per chunk slot
         self.upload_chunk_bytes = 16 << 20   # raw bytes per overlapped upload + ingest chunk
+        self.upload_middle_chunks = 4        # page-locked sources: inner chunks this many times larger
         self.kernel_timer = None        # a KernelTimer records launch durations when set
         self.bp_kernel = "staged"       # "plain": direct-gather kernel for every request
         with torch.cuda.device(self.device):
@@ -1135,8 +1136,18 @@ class SliceReconstructor:
             n_slots = 3
             while len(self._raw_pinned) < n_slots:
                 self._raw_pinned.append([None, None])        # [pinned tensor, event of its last copy]
-        for i, c0 in enumerate(range(0, k, chunk)):
-            c1 = min(k, c0 + chunk)
+        if pinned and self.upload_middle_chunks > 1 and k > 4 * chunk:
+            # the first chunk and the last two keep their size (the ingest starts early, and
+            # the filtering and summing of a large chunk is done before the last one lands,
+            # so little work is left after the transfer); the ones between are larger, so the
+            # transfer is cut into fewer copies
+            inner = k - 3 * chunk
+            n_in = -(-inner // (chunk * self.upload_middle_chunks))
+            cuts = [chunk + (inner * j) // n_in for j in range(n_in + 1)]
+            bounds = [0] + cuts + [k - chunk, k]
+        else:
+            bounds = list(range(0, k, chunk)) + [k]
+        for i, (c0, c1) in enumerate(zip(bounds[:-1], bounds[1:])):
             with torch.cuda.stream(self.copy_stream):
                 if pinned:
                     x[c0:c1].copy_(host[c0:c1], non_blocking=True)
