@@ -275,3 +275,24 @@ def test_reset_reuses_resident_records(cuda):
         got = feed(rec, order)
         for g, w in zip(got, want):
             np.testing.assert_array_equal(g, w)
+
+
+@pytest.mark.gpu
+def test_empty_calls(cuda):
+    """Zero views and zero requests are no-ops on every ingest path."""
+    import torch
+    geom = circular_cone_vectors(24, 300.0, 600.0, 16, 20, 3.0)
+    flat = np.full((1, 16, 20), 40000, np.uint16)
+    dark = np.full((1, 16, 20), 100, np.uint16)
+    none = np.zeros(0, np.int64)
+    for parker in (False, True):
+        g = geom if not parker else circular_cone_vectors(24, 300.0, 600.0, 16, 20, 3.0,
+                                                          angular_range=np.pi + 0.5)
+        rec = SliceReconstructor(None, g, verbose=False, store="bf16", filter="tc", parker=parker)
+        rec.set_flat_dark(flat, dark)
+        assert rec.add_raw_projections(none, np.zeros((0, 16, 20), np.uint16)) == 0
+        assert rec.add_raw_projections(none, torch.zeros((0, 16, 20), dtype=torch.int16).cuda()) == 0
+        assert rec.add_projections(none, np.zeros((16, 0, 20), np.float32)) == 0
+        assert rec.reconstruct_planes([]) == []
+        img, _ = rec.reconstruct_plane((0, 0, 0), (0, 0, 1), n=8)
+        assert img.shape == (8, 8) and np.all(img == 0)
