@@ -33,17 +33,18 @@ constexpr int ST_CONSUMERS = 8;               // consumer warps (one 32 x 32 til
 constexpr int ST_THREADS = 32 * (ST_CONSUMERS + 1);   // + one producer warp
 constexpr int ST_PPT = 4;                     // samples per consumer thread (i, i+4, i+8, i+12)
 constexpr int ST_BOX_H = 8;                   // rows per TMA box
-constexpr int ST_MAX_BOXES = 10;              // <= 80 staged rows per view
 constexpr int ST_CLUSTER = 4;                 // CTAs per tile, each a quarter of the views
 constexpr float MAGIC = 12582912.0f;          // 1.5 * 2^23
 constexpr int MAGIC_BITS = 0x4B400000;
 
 template <typename T> struct StageGeom;
 // Row widths (elements) are 16-byte multiples whose word pitch shifts successive rows
-// across banks (88 bf16 = 44 words, 84 f32 = 84 words).
-template <> struct StageGeom<__nv_bfloat16> { static constexpr int W = 88, ALIGN = 8, STAGES = 4; };
-template <> struct StageGeom<__half> { static constexpr int W = 88, ALIGN = 8, STAGES = 4; };
-template <> struct StageGeom<float> { static constexpr int W = 84, ALIGN = 4, STAGES = 3; };
+// across banks (88 bf16 = 44 words, 84 f32 = 84 words). MAXB boxes of 8 rows per stage:
+// FP32 stages hold 64 rows, so three CTAs fit an SM (80-row FP32 stages allowed two, and
+// the three-slice launch ran 18 % slower); taller footprints use the global-load path.
+template <> struct StageGeom<__nv_bfloat16> { static constexpr int W = 88, ALIGN = 8, STAGES = 4, MAXB = 10; };
+template <> struct StageGeom<__half> { static constexpr int W = 88, ALIGN = 8, STAGES = 4, MAXB = 10; };
+template <> struct StageGeom<float> { static constexpr int W = 84, ALIGN = 4, STAGES = 3, MAXB = 8; };
 
 enum : int { MODE_STAGED = 0, MODE_GLOBAL = 1, MODE_SKIP = 2 };
 
@@ -191,12 +192,12 @@ __device__ __forceinline__ ViewMeta view_meta(const mr_view& V, const mr_grid& g
         if (cmax < -2.f || cmin > (float)C + 1.f || rmax < -2.f || rmin > (float)R + 1.f) {
             mode = MODE_SKIP;
         } else if (cmax - cmin < (float)(W - StageGeom<T>::ALIGN - 4) &&
-                   rmax - rmin < (float)(ST_BOX_H * ST_MAX_BOXES - 4)) {
+                   rmax - rmin < (float)(ST_BOX_H * StageGeom<T>::MAXB - 4)) {
             x0 = ((int)floorf(cmin) - 1) & ~(StageGeom<T>::ALIGN - 1);
             r0 = (int)floorf(rmin) - 1;
             const int rows = (int)floorf(rmax) + 3 - r0;
             nbox = (rows + ST_BOX_H - 1) / ST_BOX_H;
-            if ((int)floorf(cmax) + 3 - x0 <= W && nbox <= ST_MAX_BOXES) mode = MODE_STAGED;
+            if ((int)floorf(cmax) + 3 - x0 <= W && nbox <= StageGeom<T>::MAXB) mode = MODE_STAGED;
         }
     }
     if (mode == MODE_STAGED) {
@@ -229,7 +230,7 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
     constexpr int W = StageGeom<T>::W;
     constexpr int S = StageGeom<T>::STAGES;
     constexpr int ESZ = (int)sizeof(T);
-    constexpr int STAGE_BYTES = W * ST_BOX_H * ST_MAX_BOXES * ESZ;
+    constexpr int STAGE_BYTES = W * ST_BOX_H * StageGeom<T>::MAXB * ESZ;
     constexpr int BOX_BYTES = W * ST_BOX_H * ESZ;
     // every TMA destination (stage start + b * BOX_BYTES) must be 128-byte aligned
     static_assert(BOX_BYTES % 128 == 0 && STAGE_BYTES % 128 == 0, "TMA box / stage not 128-byte aligned");
@@ -486,7 +487,7 @@ static int launch_staged(const mr_ring* ring, const mr_view* views, const mr_gri
     int rc = make_ring_map<T>(ring, &map);
     if (rc != MR_OK) return rc;
     constexpr int S = StageGeom<T>::STAGES;
-    const size_t smem = (size_t)S * StageGeom<T>::W * ST_BOX_H * ST_MAX_BOXES * sizeof(T) +
+    const size_t smem = (size_t)S * StageGeom<T>::W * ST_BOX_H * StageGeom<T>::MAXB * sizeof(T) +
                         (S + 32) * sizeof(ViewMeta) + 2 * S * sizeof(uint64_t) +
                         ST_CONSUMERS * 32 * sizeof(float4) + 128;
     auto kern = bp_staged_kernel<KIND, T>;
