@@ -495,6 +495,7 @@ def serving_simulation(args, dev, geom, raw_dev, flats, darks):
         f.result()
     rec.reset()
     srv.latencies.clear()
+    srv.latency_kinds.clear()
     srv.updates = 0
     t0 = time.perf_counter()
     next_req = t0 + rng.exponential(1.0 / req_rate)
@@ -522,7 +523,8 @@ def serving_simulation(args, dev, geom, raw_dev, flats, darks):
     srv.close()
     st = srv.stats()
     return {"requests": len(futs), "previews": len(previews), "batches": st["batches"],
-            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "wall_s": wall,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "slice_p50_ms": st["slice_p50_ms"],
+            "slice_p99_ms": st["slice_p99_ms"], "wall_s": wall,
             "updates_per_s": st["updates"] / wall,
             "setup": "600 raw views at 200 views/s, Poisson 500 req/s, n in {128..1024}, zoom 1-8, "
                      "COR +/-10 px, 128^3 preview per 50 views, bf16 ring, 20 GB budget"}

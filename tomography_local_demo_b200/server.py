@@ -19,7 +19,8 @@ net.py:129-154 - "slice", "preview" - rebuilt around one GPU).
 * Each request sees the views received when its batch was admitted (snapshot); the
   per-tile arithmetic and the cluster reduction order do not depend on the batch, so a
   result is bit-identical alone and in any mix.
-Latencies (submit -> result on the host) are kept in `latencies`.
+Latencies (submit -> result on the host) are kept in `latencies` (request kinds in
+`latency_kinds`).
 """
 import collections
 import threading
@@ -82,6 +83,7 @@ class SliceServer:
         self.cv = threading.Condition()
         self.in_flight = 0
         self.latencies = []
+        self.latency_kinds = []
         self.batches = 0
         self.updates = 0
         self._running = True
@@ -135,10 +137,15 @@ class SliceServer:
                 N.check(code, "slice server batch")
 
     def stats(self):
-        lat = np.array(self.latencies) * 1e3
+        """Request count, batches, updates and latency percentiles (ms) over all requests,
+        and over the slice requests alone (previews are volumes, far larger requests)."""
+        n = min(len(self.latencies), len(self.latency_kinds))     # the completer may be mid-append
+        lat = np.array(self.latencies[:n]) * 1e3
+        sl = lat[np.array(self.latency_kinds[:n]) == "slice"] if n else lat
+        pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None     # noqa: E731
         return {"requests": len(lat), "batches": self.batches, "updates": self.updates,
-                "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
-                "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None}
+                "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+                "slice_p50_ms": pct(sl, 50), "slice_p99_ms": pct(sl, 99)}
 
     # ------------------------------------------------------------------ device side
     def _free_slot(self):
@@ -258,6 +265,7 @@ class SliceServer:
                 self.cv.notify_all()
             for r, img in zip(batch, res):
                 self.latencies.append(t - r.t_submit)
+                self.latency_kinds.append(r.kind)
                 if r.kind == "slice":
                     self.updates += int(np.count_nonzero(img)) * n_views
                     r.future.set_result(img)
