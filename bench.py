@@ -19,6 +19,7 @@ collective on the data path); value = all ranks' updates / max-over-ranks time.
 """
 import argparse
 import ctypes
+import gc
 import json
 import os
 import subprocess
@@ -87,9 +88,39 @@ def as_u16(t):
 
 
 # ------------------------------------------------------------------ clocks
+def _clock_sampler_process(conn, uuid, index, period):
+    """Child process of ClockSampler: NVML samples (monotonic time, SM MHz, clock-event
+    reasons, W) every `period` s until told to stop, then all of them (read-only queries)."""
+    samples = []
+    try:
+        import pynvml as nv
+        nv.nvmlInit()
+        try:
+            h = nv.nvmlDeviceGetHandleByUUID(uuid.encode()) if uuid else nv.nvmlDeviceGetHandleByIndex(index)
+        except Exception:
+            h = nv.nvmlDeviceGetHandleByIndex(index)
+        reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        conn.send(("ready", float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))))
+        while True:
+            samples.append((time.monotonic(), float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                            int(reasons(h)), nv.nvmlDeviceGetPowerUsage(h) / 1e3))
+            if conn.poll(period):
+                conn.recv()
+                samples.append((time.monotonic(), float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                int(reasons(h)), nv.nvmlDeviceGetPowerUsage(h) / 1e3))
+                break
+        conn.send(("samples", samples))
+    except Exception as e:                 # no NVML: report unsampled
+        conn.send(("error", repr(e)))
+
+
 class ClockSampler:
-    """Samples SM clock, power and clock-event reasons every 2 ms during the timed region
-    and once at its end, through NVML (read-only queries; nothing is set)."""
+    """Samples SM clock, power and clock-event reasons every 2 ms through NVML (read-only
+    queries; nothing is set) in a child process, and keeps the samples of the timed region
+    (from mark() to the end, plus one right after it). A process of its own: NVML queries
+    in the benchmarking process held up its CUDA calls (its first queries take ~0.85 ms
+    each) and a sampling thread competes for the interpreter."""
     BITS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
             "sw_power_cap": 0x4}
 
@@ -97,65 +128,60 @@ class ClockSampler:
         self.dev = device_index
         self.samples = []
         self.max_mhz = None
-        self._stop = threading.Event()
         self.error = None
-
-    def _handle(self, nv):
-        import torch
-        try:
-            uuid = "GPU-" + str(torch.cuda.get_device_properties(self.dev).uuid)
-            return nv.nvmlDeviceGetHandleByUUID(uuid.encode())
-        except Exception:
-            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
-            idx = int(vis.split(",")[self.dev]) if vis and vis.split(",")[0].isdigit() else self.dev
-            return nv.nvmlDeviceGetHandleByIndex(idx)
-
-    def _sample(self):
-        nv, h = self._nv, self._h
-        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
-                             int(self._reasons(h)), nv.nvmlDeviceGetPowerUsage(h) / 1e3))
-
-    def _run(self):
-        try:
-            while True:
-                self._sample()
-                if self._stop.wait(0.002):
-                    break
-        except Exception as e:
-            self.error = repr(e)
+        self._proc = None
+        self._t0 = None
 
     def __enter__(self):
-        # NVML is opened before the timed region, so sampling starts with it
-        self._nv = None
+        import multiprocessing as mp
+        import torch
+        uuid = None
         try:
-            import pynvml as nv
-            nv.nvmlInit()
-            self._h = self._handle(nv)
-            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self._h, nv.NVML_CLOCK_SM))
-            self._reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
-                nv.nvmlDeviceGetCurrentClocksThrottleReasons
-            self._nv = nv
-        except Exception as e:             # no NVML: report unsampled
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(self.dev).uuid)
+        except Exception:
+            pass
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        index = int(vis.split(",")[self.dev]) if vis and vis.split(",")[0].isdigit() else self.dev
+        try:
+            ctx = mp.get_context("spawn")
+            self._conn, child = ctx.Pipe()
+            self._proc = ctx.Process(target=_clock_sampler_process, args=(child, uuid, index, 0.002), daemon=True)
+            self._proc.start()
+            if self._conn.poll(60):
+                kind, val = self._conn.recv()
+                if kind == "ready":
+                    self.max_mhz = val
+                else:
+                    self.error = val
+            else:
+                self.error = "clock sampler did not start"
+        except Exception as e:
             self.error = repr(e)
-        self.thread = threading.Thread(target=self._run if self._nv else (lambda: None), daemon=True)
-        self.thread.start()
         return self
 
     def mark(self):
-        """Start of the timed region: drop the samples taken so far. The first NVML
-        queries of a process are slow and hold up the launching thread's CUDA calls for
-        some tens of milliseconds, so the sampler is started well before the region (at
-        set-up) and only the region's own samples are kept."""
-        self.samples.clear()
+        """Start of the timed region (samples before it are dropped)."""
+        self._t0 = time.monotonic()
 
     def __exit__(self, *a):
-        self._stop.set()
-        self.thread.join(5)
-        if self._nv is not None:
-            try:
-                self._sample()             # one more right at the end of the timed region
-            except Exception as e:
-                self.error = repr(e)
+        t1 = time.monotonic()
+        if self._proc is None or self.max_mhz is None:
+            return
+        try:
+            self._conn.send("stop")
+            if self._conn.poll(30):
+                kind, val = self._conn.recv()
+                if kind == "samples":
+                    t0 = self._t0 if self._t0 is not None else t1
+                    inside = [x for x in val if t0 <= x[0] <= t1]
+                    after = [x for x in val if x[0] > t1][:1]
+                    self.samples = [x[1:] for x in inside + after]
+                else:
+                    self.error = val
+        except Exception as e:
+            self.error = repr(e)
+        finally:
+            self._proc.join(10)
 
     def summary(self):
         if not self.samples:
@@ -283,6 +309,10 @@ def run_ours(args, rank, world, local):
     rec.kernel_timer = timer
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    # the interpreter's cyclic garbage collector stays off inside the timed regions (as in
+    # timeit): a full collection is a pause of the launching thread unrelated to the path
+    gc.collect()
+    gc.disable()
     clocks.mark()
     e0.record(rec.ingest_stream)
     for _ in range(args.steps):
@@ -290,6 +320,7 @@ def run_ours(args, rank, world, local):
     e1.record(rec.stream)
     torch.cuda.synchronize()
     clocks.__exit__(None, None, None)
+    gc.enable()
     barrier(world)
     rec.kernel_timer = None
     t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3, world, dev)
@@ -311,11 +342,15 @@ def run_ours(args, rank, world, local):
         step_e2e()
     torch.cuda.synchronize()
     barrier(world)
+    gc.collect()
+    gc.disable()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         step_e2e()
     torch.cuda.synchronize()
-    t_e2e = max_over_ranks(time.perf_counter() - t0, world, dev)
+    t_e2e_local = time.perf_counter() - t0
+    gc.enable()
+    t_e2e = max_over_ranks(t_e2e_local, world, dev)
     h2d = raw_host.numel() * 2 + V * (64 + 32) + len(reqs) * 256
     d2h = sum(r["n"] ** 2 for r in reqs) * 8         # the images come back as float64
 

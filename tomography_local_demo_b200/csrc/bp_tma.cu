@@ -21,6 +21,7 @@
 
 #include <cooperative_groups.h>
 #include <mutex>
+#include <type_traits>
 
 #include "mr_common.cuh"
 
@@ -90,6 +91,22 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
         : "memory");
+}
+
+__device__ __forceinline__ unsigned short lds_u16(uint32_t addr) {
+    unsigned short u;
+    asm volatile("ld.shared.u16 %0, [%1];" : "=h"(u) : "r"(addr));
+    return u;
+}
+// a - c, rounded to nearest, for a 16-bit value a (raw BF16 / FP16 bits) and an FP32 c
+template <typename T>
+__device__ __forceinline__ float sub16_f32(unsigned short a, float c) {
+    float d;
+    if constexpr (std::is_same<T, __nv_bfloat16>::value)
+        asm("sub.rn.f32.bf16 %0, %1, %2;" : "=f"(d) : "h"(a), "f"(c));
+    else
+        asm("sub.rn.f32.f16 %0, %1, %2;" : "=f"(d) : "h"(a), "f"(c));
+    return d;
 }
 
 template <typename T>
@@ -389,12 +406,24 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                                        (uint32_t)__float_as_int(yc) * (uint32_t)ESZ - kofs;
                         off = min(off, maxoff);
                         const uint32_t a = base + off;
-                        const float q00 = lds_elem<T>(a);
-                        const float q01 = lds_elem<T>(a + ESZ);
-                        const float q10 = lds_elem<T>(a + W * ESZ);
-                        const float q11 = lds_elem<T>(a + W * ESZ + ESZ);
-                        const float ta = fmaf(fc, q01 - q00, q00);
-                        const float tb = fmaf(fc, q11 - q10, q10);
+                        float ta, tb;
+                        if constexpr (sizeof(T) == 2) {
+                            // the right taps stay 16-bit: one mixed-precision subtraction each
+                            // (16-bit values widen exactly, so it is the FP32 difference) instead
+                            // of a widening and an FP32 subtraction
+                            const unsigned short u01 = lds_u16(a + ESZ), u11 = lds_u16(a + W * ESZ + ESZ);
+                            const float q00 = lds_elem<T>(a);
+                            const float q10 = lds_elem<T>(a + W * ESZ);
+                            ta = fmaf(fc, sub16_f32<T>(u01, q00), q00);
+                            tb = fmaf(fc, sub16_f32<T>(u11, q10), q10);
+                        } else {
+                            const float q00 = lds_elem<T>(a);
+                            const float q01 = lds_elem<T>(a + ESZ);
+                            const float q10 = lds_elem<T>(a + W * ESZ);
+                            const float q11 = lds_elem<T>(a + W * ESZ + ESZ);
+                            ta = fmaf(fc, q01 - q00, q00);
+                            tb = fmaf(fc, q11 - q10, q10);
+                        }
                         const float val = fmaf(fr, tb - ta, ta);
                         acc[p] = fmaf(KIND == MR_CONE ? r * r : m.cu.w, val, acc[p]);
                     }
