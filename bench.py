@@ -516,16 +516,17 @@ def serving_simulation(args, dev, geom, raw_dev, flats, darks):
     import torch
     from tomography_local_demo_b200 import SliceReconstructor
     from tomography_local_demo_b200.server import SliceServer
-    from tomography_local_demo_b200.stream import arrival_order
+    from tomography_local_demo_b200.stream import AcquisitionSchedule
     rec = SliceReconstructor(None, geom, store="bf16", verbose=False, device=dev, filter=args.filter)
     rec.set_flat_dark(as_u16(flats), as_u16(darks))
     srv = SliceServer(rec, budget_bytes=20e9, max_batch=128, pool_bytes=1 << 30)
     rng = np.random.default_rng(5)
     V, rate, req_rate = WORKLOAD["views"], 200.0, 500.0
-    order = arrival_order(V, "interleaved")
+    sched = AcquisitionSchedule(V, "interleaved", group=10, rate=rate)
     futs, previews = [], []
     # warm the server (first replay captures the graphs)
-    rec.add_raw_projections(order[:10], raw_dev[torch.from_numpy(order[:10]).to(dev)])
+    first = sched.groups[0]
+    rec.add_raw_projections(first, raw_dev[torch.from_numpy(first).to(dev)])
     for f in [srv.submit((0, 0, 0), (0, 0, 1), n=n) for n in (128, 1024)] + [srv.submit_preview(128)]:
         f.result()
     rec.reset()
@@ -534,14 +535,13 @@ def serving_simulation(args, dev, geom, raw_dev, flats, darks):
     srv.updates = 0
     t0 = time.perf_counter()
     next_req = t0 + rng.exponential(1.0 / req_rate)
-    sent = 0
-    while sent < V:
-        now = time.perf_counter()
-        due = int(min(V, (now - t0) * rate // 10 * 10 + 10))
-        if due > sent:
-            idx = order[sent:due]
+    pushed, sent = 0, 0                 # groups and views pushed so far
+    while pushed < len(sched):
+        due = sched.due_by(time.perf_counter() - t0)
+        if due > pushed:
+            idx = np.concatenate(sched.groups[pushed:due])
             rec.add_raw_projections(idx, raw_dev[torch.from_numpy(idx).to(dev)])
-            before, sent = sent, due
+            before, sent, pushed = sent, sent + len(idx), due
             if sent // 50 > before // 50:
                 previews.append(srv.submit_preview(128))
         while next_req <= time.perf_counter():

@@ -36,6 +36,8 @@ extern "C" {
 #define MR_ERR_TIMEOUT      -4   /* a bounded device-side wait gave up */
 #define MR_ERR_SCRATCH_LIMIT -5  /* the request needs more than the library's fixed device
                                     scratch (mr_backproject_persistent_noalloc) */
+#define MR_ERR_CAPTURE      -6   /* the first call of mr_backproject_persistent_noalloc on a
+                                    device came while its stream was being captured */
 
 /* ---- element types ------------------------------------------------------------- */
 #define MR_F32   0
@@ -193,7 +195,11 @@ int mr_backproject_persistent(const mr_ring* ring, const mr_view* views_dev,
  * and output. The counter is zeroed on `stream` by each call.
  *   - The device that owns `stream` must be the current device.
  *   - The first call on a device looks up the array's device address (and may load the
- *     library's device code); make that first call before any stream capture.
+ *     library's device code); make that first call before any stream capture. A first
+ *     call on a stream that is being captured returns MR_ERR_CAPTURE and launches nothing.
+ *   - The address is kept for the life of the process. After cudaDeviceReset (or a
+ *     reset of the primary context by the host application) the array may move: do not
+ *     call this entry point again in that process.
  *   - Every call on a device shares the one counter: calls that overlap on the GPU race
  *     and give wrong results. Order them on one stream (or wait between them).
  *   - max_tiles above MR_NOALLOC_MAX_TILES (the range one 32-bit counter can hand out)

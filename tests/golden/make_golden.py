@@ -1,9 +1,10 @@
 """Generate the golden fixtures of tests/golden/ by running the REFERENCE itself.
 
-    python tests/golden/make_golden.py [path-to-reference-checkout]
+    python tests/golden/make_golden.py PATH-TO-REFERENCE-CHECKOUT [--net-only]
+    MINIRECAST_REF=PATH-TO-REFERENCE-CHECKOUT python tests/golden/make_golden.py
 
-Imports minirecast (ZYHuang216/Tomography-local-demo) from the given checkout
-(default /root/reference), runs its own functions on small seeded inputs and writes
+Imports minirecast (ZYHuang216/Tomography-local-demo) from the checkout given as the
+argument or in the MINIRECAST_REF environment variable (one of them is required), runs its own functions on small seeded inputs and writes
 compressed .npz fixtures next to this script. The tests only read the .npz files; the
 reference is not needed to run them. Numba's cache goes to a temporary directory so a
 read-only checkout works.
@@ -245,7 +246,10 @@ def loader_fixtures(FX, H5, save):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    root = args[0] if args else "/root/reference"
+    root = args[0] if args else os.environ.get("MINIRECAST_REF")
+    if not root or not os.path.isdir(os.path.join(root, "minirecast")):
+        sys.exit("usage: make_golden.py PATH-TO-REFERENCE-CHECKOUT [--net-only] "
+                 "(or set MINIRECAST_REF): the directory that holds the minirecast package")
     if "--net-only" in sys.argv:                 # only net_frames.npz
         os.environ.setdefault("NUMBA_CACHE_DIR", tempfile.mkdtemp(prefix="numba_cache_"))
         sys.path.insert(0, root)

@@ -264,3 +264,56 @@ def test_band_ordered_tiles_are_a_permutation_sorted_by_height():
     pts = grids.copy()
     pts["flags"][1] = N.MR_GRID_POINTS
     assert N.plan_tiles(pts, axis).tobytes() == N.plan_tiles(pts).tobytes()
+
+
+def test_product_phantom_matches_reference():
+    """The torch chord-length projectors of the product phantom reproduce the reference's
+    own phantom outputs (densities, line integrals, parallel and cone projections)."""
+    import torch
+    from tomography_local_demo_b200 import phantom as PH
+    g = golden("phantom.npz")
+    ph = PH.EllipsoidPhantom(scale=50.0)
+    np.testing.assert_allclose(ph.evaluate(g["pts"]), g["evaluate"], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(ph.line_integrals(g["starts"], g["dirs"]), g["lines"], rtol=1e-12, atol=1e-12)
+    pg = G.ParallelGeometry(np.arange(9) * np.pi / 9, 10, 12, 9.0, 11.0)
+    par = PH.project_parallel_torch(ph, pg).numpy()
+    assert par.shape == g["par"].shape and par.dtype == np.float32
+    np.testing.assert_allclose(par, g["par"], rtol=1e-6, atol=1e-6 * np.abs(g["par"]).max())
+    cg = G.circular_cone_vectors(9, 300.0, 600.0, 10, 12, 15.0, det_shift_u=1.5)
+    cone = PH.project_cone_torch(ph, cg, device="cpu").permute(1, 0, 2).numpy()
+    np.testing.assert_allclose(cone, g["cone"], rtol=1e-6, atol=1e-6 * np.abs(g["cone"]).max())
+    assert torch.get_default_dtype() == torch.float32
+
+
+def test_acquisition_schedule_and_feeder():
+    """Groups in arrival order, group k due when the views before it are (rate views/s),
+    all at once for rate <= 0; the Feeder pushes every view once, in that order, and a
+    stop() ends it before the next group."""
+    sc = S.AcquisitionSchedule(10, "interleaved", group=4, rate=8.0)
+    assert [len(g) for g in sc.groups] == [4, 4, 2]
+    np.testing.assert_array_equal(np.concatenate(sc.groups), S.arrival_order(10, "interleaved"))
+    np.testing.assert_allclose(sc.due, [0.0, 0.5, 1.0])
+    assert [sc.due_by(t) for t in (0.0, 0.49, 0.5, 0.99, 5.0)] == [1, 1, 2, 2, 3]
+    assert (S.AcquisitionSchedule(5, group=2, rate=0).due == 0).all()
+    assert list(S.arrival_order(1, "interleaved")) == [0] and len(S.arrival_order(0, "interleaved")) == 0
+
+    class Sink:
+        def __init__(self):
+            self.calls = []
+
+        def add_projections(self, idx, block):
+            self.calls.append((np.array(idx), np.array(block)))
+
+    proj = np.arange(3 * 7 * 2, dtype=np.float32).reshape(3, 7, 2)
+    sink = Sink()
+    f = S.Feeder(sink, proj, order="interleaved", group=3, rate=0, verbose=False)
+    f.run()
+    assert f.sent == 7 and [len(i) for i, _ in sink.calls] == [3, 3, 1]
+    for idx, blk in sink.calls:
+        np.testing.assert_array_equal(blk, proj[:, idx, :])
+    slow = Sink()
+    f = S.Feeder(slow, proj, group=1, rate=2.0, verbose=False)
+    f.start()
+    f.stop()
+    f.join(5)
+    assert not f.is_alive() and f.stopped and len(slow.calls) <= 1

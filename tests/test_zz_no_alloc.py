@@ -44,14 +44,18 @@ def _batch(box, reqs):
     return grids, N.plan_tiles(grids), off
 
 
-def _run(lib, dr, grids, tiles, n_out, noalloc):
+def _run(lib, dr, grids, tiles, n_out, noalloc, stream=None):
+    """One persistent launch through the C ABI on `stream` (a torch stream, or None for
+    the legacy default stream, passed as NULL)."""
     dev = dr.dev
     g_dev = R._struct_tensor(grids, dev)
     t_dev = R._struct_tensor(tiles, dev)
     nt_dev = torch.tensor([len(tiles)], dtype=torch.int64, device=dev)
     out = torch.full((n_out,), float("nan"), dtype=torch.float32, device=dev)
     status = torch.zeros(1, dtype=torch.int32, device=dev)
-    st = V(torch.cuda.current_stream(dev).cuda_stream)
+    if stream is not None:
+        stream.wait_stream(torch.cuda.current_stream(dev))
+    st = V(stream.cuda_stream) if stream is not None else None
     max_tiles = len(tiles) + 7
     if noalloc:
         rc = lib.mr_backproject_persistent_noalloc(dr.c, V(dr.views.data_ptr()), V(g_dev.data_ptr()),
@@ -68,7 +72,8 @@ def _run(lib, dr, grids, tiles, n_out, noalloc):
     return out.cpu().numpy()
 
 
-def test_noalloc_matches_persistent_on_two_calls_in_a_row(ring):
+@pytest.mark.parametrize("stream_kind", ["side", "null"])
+def test_noalloc_matches_persistent_on_two_calls_in_a_row(ring, stream_kind):
     dr, box = ring
     lib = N.load()
     batches = [
@@ -78,8 +83,9 @@ def test_noalloc_matches_persistent_on_two_calls_in_a_row(ring):
     ]
     for reqs in batches:
         grids, tiles, n_out = _batch(box, reqs)
-        want = _run(lib, dr, grids, tiles, n_out, noalloc=False)
-        got = _run(lib, dr, grids, tiles, n_out, noalloc=True)
+        stream = torch.cuda.Stream(dr.dev) if stream_kind == "side" else None
+        want = _run(lib, dr, grids, tiles, n_out, noalloc=False, stream=stream)
+        got = _run(lib, dr, grids, tiles, n_out, noalloc=True, stream=stream)
         assert np.isfinite(want).all() and np.count_nonzero(want) > 0
         # the same kernel and reduction order: bit-identical, as the server's tests require
         np.testing.assert_array_equal(got, want)
@@ -95,3 +101,21 @@ def test_noalloc_rejects_work_beyond_its_scratch(ring):
     assert b"scratch" in lib.mr_status_string(rc)
     assert lib.mr_backproject_persistent_noalloc(dr.c, fake, fake, fake, None, 16, fake, None,
                                                  None) == N.MR_ERR_INVALID
+
+
+def test_noalloc_rejects_a_stream_of_another_device(ring):
+    """The stream's device must be the current device: a stream of another GPU is refused
+    on the host before anything is launched (needs two GPUs)."""
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    dr, box = ring
+    lib = N.load()
+    grids, tiles, n_out = _batch(box, [((0, 0, 0), (0.0, 0.0, 1.0), 32, 1.0, 0.0)])
+    other = (dr.dev.index or 0) + 1
+    with torch.cuda.device(other):
+        foreign = torch.cuda.Stream(other)
+    fake = V(1 << 20)          # never dereferenced: the device check fails before any launch
+    with torch.cuda.device(dr.dev):
+        rc = lib.mr_backproject_persistent_noalloc(dr.c, fake, fake, fake, fake, len(tiles), fake, None,
+                                                   V(foreign.cuda_stream))
+    assert rc == N.MR_ERR_INVALID

@@ -17,6 +17,7 @@ MR_ERR_CUDA = -2
 MR_ERR_UNSUPPORTED = -3
 MR_ERR_TIMEOUT = -4
 MR_ERR_SCRATCH_LIMIT = -5
+MR_ERR_CAPTURE = -6
 MR_NOALLOC_MAX_TILES = 1 << 31
 
 MR_F32, MR_BF16, MR_F16, MR_U16 = 0, 1, 2, 3

@@ -636,6 +636,15 @@ int noalloc_counter(cudaStream_t stream, unsigned int** counter) {
     }
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_addr[dev]) {
+        // the symbol lookup may load device code, which a capture in progress forbids
+        if (stream) {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+                cudaGetLastError();
+                return MR_ERR_CUDA;
+            }
+            if (cs != cudaStreamCaptureStatusNone) return MR_ERR_CAPTURE;
+        }
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
             cudaGetLastError();

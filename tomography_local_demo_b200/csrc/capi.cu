@@ -20,6 +20,8 @@ extern "C" const char* mr_status_string(int status) {
         case MR_ERR_UNSUPPORTED: return "unsupported configuration";
         case MR_ERR_TIMEOUT: return "device-side wait timed out";
         case MR_ERR_SCRATCH_LIMIT: return "request exceeds the fixed device scratch of the no-allocation entry point";
+        case MR_ERR_CAPTURE:
+            return "first no-allocation call on this device came during stream capture; make it before capturing";
         default: return "unknown status";
     }
 }

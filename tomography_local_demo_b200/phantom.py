@@ -1,16 +1,22 @@
-"""Analytic ellipsoid phantoms (the data model of minirecast phantom.py) and synthetic
-acquisitions.
+"""Analytic ellipsoid phantoms and synthetic acquisitions, evaluated with torch in FP64.
 
-Every ellipsoid has an exact line integral, so simulated projections carry no
-discretisation error. Besides the reference's NumPy API (EllipsoidPhantom,
-project_parallel, project_cone), `project_cone_torch` evaluates the same integrals in
-FP64 with torch on any device, which makes full-size cone acquisitions (600 views of
-384 x 486) take seconds on a GPU, and `raw_counts` turns line integrals into uint16
-detector counts with flat/dark fields and Poisson noise.
+The phantom data model is minirecast's (phantom.py:11-37: a table of constant-density
+ellipsoids, value, semi-axes, centre, rotation about z, scaled to mm). Every ellipsoid
+has an exact line integral, so simulated projections carry no discretisation error.
+
+All evaluation goes through one routine, `chord_integrals`: an ellipsoid maps to the unit
+sphere under y = M (x - c), so a line x = p + t w meets it where |M(p - c) + t M w| <= 1,
+a quadratic in t whose root distance, times |w| = 1, is the chord length; the integral
+is the density times the chord. The chord of the whole line does not depend on where
+along the line p sits, so projectors take p on the detector (or the source) directly.
+The projectors run batched on any torch device: a full cone acquisition of 600 views of
+384 x 486 takes seconds on a GPU. `raw_counts` turns line integrals into uint16 detector
+counts with flat / dark fields and Poisson noise.
 """
 import numpy as np
 
-# value, a, b, c, x0, y0, z0, phi (deg, about z) - modified 3D Shepp-Logan (phantom.py:11-22)
+# value, a, b, c, x0, y0, z0, phi (deg, about z): the modified 3D Shepp-Logan table of
+# minirecast phantom.py:11-22 (a constant: the same phantom must come out)
 MODIFIED_SHEPP_LOGAN = np.array([
     [1.0, .6900, .920, .810, 0.00, 0.0000, 0.00, 0],
     [-0.8, .6624, .874, .780, 0.00, -0.0184, 0.00, 0],
@@ -25,46 +31,67 @@ MODIFIED_SHEPP_LOGAN = np.array([
 ])
 
 
-def _frames(table, scale):
-    """(values, centres, M) with M (x - c) mapping each ellipsoid to the unit sphere."""
-    vals, cents, mats = [], [], []
-    for v, a, b, c, x0, y0, z0, phi in np.asarray(table, float):
-        p = np.deg2rad(phi)
-        rot = np.array([[np.cos(p), -np.sin(p), 0.0], [np.sin(p), np.cos(p), 0.0], [0.0, 0.0, 1.0]])
-        mats.append(np.diag(1.0 / (scale * np.array([a, b, c]))) @ rot.T)
-        vals.append(v)
-        cents.append(scale * np.array([x0, y0, z0]))
-    return np.array(vals), np.array(cents), np.array(mats)
-
-
 class EllipsoidPhantom:
-    """Sum of constant-density ellipsoids, coordinates in mm (phantom.py:40-70)."""
+    """Sum of constant-density ellipsoids, coordinates in mm.
+
+    Per ellipsoid e: density vals[e], centre centers[e] (mm) and the 3x3 map mats[e]
+    taking x - centre to the unit sphere (inverse scaled semi-axes after the inverse
+    rotation about z)."""
 
     def __init__(self, scale=1.0, table=MODIFIED_SHEPP_LOGAN):
         self.scale = float(scale)
-        self.table = np.asarray(table, float)
-        self.vals, self.centers, self.mats = _frames(self.table, self.scale)
+        self.table = np.asarray(table, float).reshape(-1, 8)
+        t = self.table
+        phi = np.deg2rad(t[:, 7])
+        cos, sin = np.cos(phi), np.sin(phi)
+        inv_axes = 1.0 / (self.scale * t[:, 1:4])
+        # rows of R^T scaled by the inverse semi-axes: M = diag(1/axes) R^T
+        rt = np.zeros((len(t), 3, 3))
+        rt[:, 0, 0], rt[:, 0, 1] = cos, sin
+        rt[:, 1, 0], rt[:, 1, 1] = -sin, cos
+        rt[:, 2, 2] = 1.0
+        self.mats = inv_axes[:, :, None] * rt
+        self.vals = t[:, 0].copy()
+        self.centers = self.scale * t[:, 4:7]
+
+    def _tensors(self, device):
+        import torch
+        f64 = dict(dtype=torch.float64, device=device)
+        return (torch.as_tensor(self.vals, **f64), torch.as_tensor(self.centers, **f64),
+                torch.as_tensor(self.mats, **f64))
 
     def evaluate(self, points):
-        pts = np.asarray(points, dtype=np.float64)
-        out = np.zeros(pts.shape[:-1])
-        for v, c, M in zip(self.vals, self.centers, self.mats):
-            y = (pts - c) @ M.T
-            out += v * (np.einsum("...i,...i->...", y, y) <= 1.0)
-        return out
+        """Density at points [..., 3] (mm) -> float64 array [...]."""
+        import torch
+        pts = torch.as_tensor(np.asarray(points, np.float64))
+        vals, cents, mats = self._tensors(pts.device)
+        y = torch.einsum("eij,...ej->...ei", mats, pts[..., None, :] - cents)
+        inside = (y * y).sum(-1) <= 1.0
+        return (inside.double() * vals).sum(-1).numpy()
 
     def line_integrals(self, starts, dirs):
-        """Exact integrals along start + t dir (unit dirs), shape (..., 3) -> (...)."""
-        starts = np.asarray(starts, np.float64)
-        dirs = np.asarray(dirs, np.float64)
-        out = np.zeros(np.broadcast_shapes(starts.shape, dirs.shape)[:-1])
-        for v, c, M in zip(self.vals, self.centers, self.mats):
-            p, q = (starts - c) @ M.T, dirs @ M.T
-            qq = np.einsum("...i,...i->...", q, q)
-            pq = np.einsum("...i,...i->...", p, q)
-            pp = np.einsum("...i,...i->...", p, p)
-            out += v * 2.0 * np.sqrt(np.clip(pq * pq - qq * (pp - 1.0), 0.0, None)) / qq
-        return out
+        """Exact integrals along the lines start + t dir (unit dirs), [..., 3] -> [...]."""
+        import torch
+        return chord_integrals(self, torch.as_tensor(np.asarray(starts, np.float64)),
+                               torch.as_tensor(np.asarray(dirs, np.float64))).numpy()
+
+
+def chord_integrals(phantom, points, dirs):
+    """Line integrals of `phantom` along the full lines through `points` with unit
+    directions `dirs` (torch float64 tensors, broadcastable [..., 3]) -> float64 [...]."""
+    import torch
+    vals, cents, mats = phantom._tensors(points.device)
+    shape = torch.broadcast_shapes(points.shape, dirs.shape)[:-1]
+    acc = torch.zeros(shape, dtype=torch.float64, device=points.device)
+    for e in range(len(vals)):
+        a = (points - cents[e]) @ mats[e].T            # foot of the line in sphere space
+        b = dirs @ mats[e].T                           # direction in sphere space
+        bb = (b * b).sum(-1)
+        ab = (a * b).sum(-1)
+        # |a + t b|^2 = 1  ->  roots t = (-ab +- sqrt(ab^2 - bb (|a|^2 - 1))) / bb
+        disc = ab * ab - bb * ((a * a).sum(-1) - 1.0)
+        acc += vals[e] * 2.0 * torch.sqrt(disc.clamp(min=0.0)) / bb
+    return acc
 
 
 def random_ellipsoids(n, seed, mu_range=(0.01, 0.2), axes_range=(2.0, 25.0), radius=30.0):
@@ -84,64 +111,44 @@ def random_ellipsoids(n, seed, mu_range=(0.01, 0.2), axes_range=(2.0, 25.0), rad
     return np.array(rows)
 
 
-def project_parallel(phantom, geom):
-    """Analytic parallel-beam projections [rows, angles, cols] float32 (phantom.py:73-83)."""
-    u, v = geom.detector_coords()
-    data = np.empty((geom.rows, len(geom.angles), geom.cols), dtype=np.float32)
-    ez = np.array([0.0, 0.0, 1.0])
-    for k, th in enumerate(geom.angles):
-        d = np.array([np.cos(th), np.sin(th), 0.0])
-        eu = np.array([-np.sin(th), np.cos(th), 0.0])
-        starts = u[None, :, None] * eu + v[:, None, None] * ez - 10.0 * phantom.scale * d
-        data[:, k, :] = phantom.line_integrals(starts, d)
-    return data
-
-
-def project_cone(phantom, geom):
-    """Analytic cone-beam projections [rows, angles, cols] float32 (phantom.py:86-98)."""
-    R, C = geom.rows, geom.cols
-    cc = np.arange(C) - (C - 1) / 2.0
-    rr = np.arange(R) - (R - 1) / 2.0
-    data = np.empty((R, geom.n_angles, C), dtype=np.float32)
-    for k, vec in enumerate(geom.vectors):
-        s, d, u, v = vec[0:3], vec[3:6], vec[6:9], vec[9:12]
-        dirs = d + cc[None, :, None] * u + rr[:, None, None] * v - s
-        dirs /= np.linalg.norm(dirs, axis=-1, keepdims=True)
-        data[:, k, :] = phantom.line_integrals(s[None, None, :], dirs)
-    return data
-
-
 def project_cone_torch(phantom, geom, device="cuda", views_per_batch=16):
-    """The same integrals as project_cone, FP64 on a torch device.
-    Returns a float32 tensor [angles, rows, cols] on that device."""
+    """Cone-beam line integrals of `phantom` for a ConeVecGeometry (ASTRA vectors: the ray
+    of detector pixel (r, c) runs from the source s to d + (c - (C-1)/2) u + (r - (R-1)/2) v).
+    FP64 on a torch device; returns a float32 tensor [angles, rows, cols] there."""
     import torch
     dev = torch.device(device)
     R, C = geom.rows, geom.cols
-    V = torch.as_tensor(np.asarray(geom.vectors), dtype=torch.float64, device=dev)
+    vec = torch.as_tensor(np.asarray(geom.vectors), dtype=torch.float64, device=dev)
     cc = torch.arange(C, dtype=torch.float64, device=dev) - (C - 1) / 2.0
     rr = torch.arange(R, dtype=torch.float64, device=dev) - (R - 1) / 2.0
-    vals = torch.as_tensor(phantom.vals, dtype=torch.float64, device=dev)
-    cents = torch.as_tensor(phantom.centers, dtype=torch.float64, device=dev)
-    mats = torch.as_tensor(phantom.mats, dtype=torch.float64, device=dev)
-    out = torch.empty((len(V), R, C), dtype=torch.float32, device=dev)
-    for k0 in range(0, len(V), views_per_batch):
-        vb = V[k0:k0 + views_per_batch]
-        s, d, u, v = vb[:, 0:3], vb[:, 3:6], vb[:, 6:9], vb[:, 9:12]
-        pix = (d[:, None, None, :] + cc[None, None, :, None] * u[:, None, None, :]
-               + rr[None, :, None, None] * v[:, None, None, :])
-        dirs = pix - s[:, None, None, :]
-        dirs = dirs / torch.linalg.norm(dirs, dim=-1, keepdim=True)
-        acc = torch.zeros(dirs.shape[:-1], dtype=torch.float64, device=dev)
-        for e in range(len(vals)):
-            M = mats[e]
-            p = (s - cents[e]) @ M.T                       # [b, 3]
-            q = dirs @ M.T                                 # [b, R, C, 3]
-            qq = (q * q).sum(-1)
-            pq = (q * p[:, None, None, :]).sum(-1)
-            pp = (p * p).sum(-1)[:, None, None]
-            acc += vals[e] * 2.0 * torch.sqrt(torch.clamp(pq * pq - qq * (pp - 1.0), min=0.0)) / qq
-        out[k0:k0 + len(vb)] = acc.to(torch.float32)
+    out = torch.empty((len(vec), R, C), dtype=torch.float32, device=dev)
+    for k0 in range(0, len(vec), views_per_batch):
+        vb = vec[k0:k0 + views_per_batch, None, None, :]          # [b, 1, 1, 12]
+        src = vb[..., 0:3]
+        pix = vb[..., 3:6] + cc[:, None] * vb[..., 6:9] + rr[:, None, None] * vb[..., 9:12]
+        ray = pix - src
+        ray = ray / torch.linalg.norm(ray, dim=-1, keepdim=True)
+        out[k0:k0 + len(vb)] = chord_integrals(phantom, src, ray).to(torch.float32)
     return out
+
+
+def project_parallel_torch(phantom, geom, device="cpu"):
+    """Parallel-beam line integrals for a ParallelGeometry: the ray of angle th and detector
+    pixel (r, c) has direction (cos th, sin th, 0) and passes through u (-sin th, cos th, 0)
+    + v (0, 0, 1), u and v the pixel's detector coordinates. Returns float32 [rows, angles,
+    cols] (the layout of the reference's projection blocks) on `device`."""
+    import torch
+    dev = torch.device(device)
+    u, v = geom.detector_coords()
+    u = torch.as_tensor(u, dtype=torch.float64, device=dev)
+    v = torch.as_tensor(v, dtype=torch.float64, device=dev)
+    th = torch.as_tensor(np.asarray(geom.angles, np.float64), device=dev)
+    zero = torch.zeros_like(th)
+    ray = torch.stack([torch.cos(th), torch.sin(th), zero], -1)            # [A, 3]
+    across = torch.stack([-torch.sin(th), torch.cos(th), zero], -1)        # [A, 3]
+    foot = (u[None, None, :, None] * across[None, :, None, :]
+            + v[:, None, None, None] * torch.tensor([0.0, 0.0, 1.0], dtype=torch.float64, device=dev))
+    return chord_integrals(phantom, foot, ray[None, :, None, :]).to(torch.float32)
 
 
 def raw_counts(line_integrals, flat, dark, seed=0):
