@@ -226,17 +226,16 @@ def max_over_ranks(x, world, device=None):
 
 
 # ------------------------------------------------------------------ CPU legs (oracle)
-def cpu_job(raw_u16, flats_u16, darks_u16, geom, reqs, box, precision="ref", pixel_stride=1,
-            view_limit=None, threads=None):
-    """The reference's CPU algorithm (oracle port): correction, FDK filter, then the
-    slices' in-box pixels (every `pixel_stride`-th) back-projected from all views.
-    Returns (images-or-values, timings dict)."""
+def cpu_job(raw_u16, flats_u16, darks_u16, geom, reqs, box, precision="ref", threads=None):
+    """The reference's CPU algorithm (oracle port): correction, FDK filter, then every
+    in-box pixel of the slices back-projected from all views.
+    Returns ([(mask, values) per slice], timings dict)."""
     from concurrent.futures import ThreadPoolExecutor
     from oracle import bp as obp
     from oracle import filter as of
     threads = threads or os.cpu_count()
     obp.threads(threads)
-    A = raw_u16.shape[0] if view_limit is None else view_limit
+    A = raw_u16.shape[0]
     t0 = time.perf_counter()
     d_b = np.mean([of.bin_mean(f, 1) for f in darks_u16], axis=0)
     f_b = np.mean([of.bin_mean(f, 1) for f in flats_u16], axis=0)
@@ -258,9 +257,7 @@ def cpu_job(raw_u16, flats_u16, darks_u16, geom, reqs, box, precision="ref", pix
     from oracle import geometry as og
     vals, n_upd, t_bp = [], 0, 0.0
     for r in reqs:
-        pts, mask = og.slice_points(box, r["origin"], r["normal"], r["n"])
-        sel = np.zeros_like(mask)
-        sel[::pixel_stride] = mask[::pixel_stride]
+        pts, sel = og.slice_points(box, r["origin"], r["normal"], r["n"])
         P = pts[sel]
         t1 = time.perf_counter()
         v = obp.bp_cone(q[:A], K["s"][:A], K["d"][:A], K["uu"][:A], K["vv"][:A], K["n"][:A],
@@ -269,12 +266,6 @@ def cpu_job(raw_u16, flats_u16, darks_u16, geom, reqs, box, precision="ref", pix
         n_upd += len(P) * A
         vals.append((sel, v))
     return vals, dict(t_filter=t_filter, views=A, t_bp=t_bp, updates=n_upd, threads=threads)
-
-
-def cpu_rate(timing, total_updates, total_views):
-    """Whole-job updates/s extrapolated from a sample (filter per view, BP per update)."""
-    t_job = timing["t_filter"] / timing["views"] * total_views + timing["t_bp"] / timing["updates"] * total_updates
-    return total_updates / t_job, t_job
 
 
 # ------------------------------------------------------------------ our arm
@@ -565,21 +556,35 @@ def serving_simulation(args, dev, geom, raw_dev, flats, darks):
                      "COR +/-10 px, 128^3 preview per 50 views, bf16 ring, 20 GB budget"}
 
 
+def cpu_whole_job(raw, fl, dk, geom, reqs, box, reps, warmup=1, precision="ref"):
+    """Time the whole job on the host with the oracle port: correction + FDK filter of all
+    views, then every in-box pixel of every slice back-projected from all views. Returns
+    (per-run job seconds, timings of the last run, values of the last run)."""
+    for _ in range(warmup):
+        cpu_job(raw, fl, dk, geom, reqs, box, precision)
+    runs, tm, vals = [], None, None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        vals, tm = cpu_job(raw, fl, dk, geom, reqs, box, precision)
+        runs.append(time.perf_counter() - t0)
+    return runs, tm, vals
+
+
 def cpu_baseline_and_accuracy(args, geom, raw_dev, flats, darks, reqs, box, updates, imgs):
     raw = as_u16(raw_dev)
     fl, dk = as_u16(flats), as_u16(darks)
     V = WORKLOAD["views"]
-    stride = 8
-    _, tm = cpu_job(raw, fl, dk, geom, reqs, box, "ref", pixel_stride=stride)
-    rate, t_job = cpu_rate(tm, updates, V)
-    base = {"value": rate, "unit": "updates/s", "cores": tm["threads"], "kind": "port",
-            "sample": (f"oracle port (C back-projection, NumPy filter) on {tm['threads']} host threads: "
-                       f"correction+filter of all {V} views ({tm['t_filter']:.2f} s) and every "
-                       f"{stride}th row of the 3 slices' in-box pixels x {V} views ({tm['t_bp']:.2f} s); "
-                       f"whole job extrapolated to {t_job:.1f} s")}
+    runs, tm, _ = cpu_whole_job(raw, fl, dk, geom, reqs, box, reps=3)
+    t_job = float(np.median(runs))
+    base = {"value": updates / t_job, "unit": "updates/s", "cores": tm["threads"], "kind": "port",
+            "sample": (f"the whole job, measured (median of {len(runs)} runs after 1 warm-up): oracle port "
+                       f"(C back-projection with FP64 accumulation, NumPy FDK filter) on {tm['threads']} host "
+                       f"threads, correction + filter of all {V} views ({tm['t_filter']:.2f} s) and every "
+                       f"in-box pixel of the 3 slices x {V} views ({tm['t_bp']:.2f} s); job "
+                       f"{t_job:.2f} s (runs {', '.join(f'{r:.2f}' for r in runs)} s)")}
     acc = {}
     if imgs is not None:
-        vals64, _ = cpu_job(raw, fl, dk, geom, reqs, box, "fp64", pixel_stride=stride)
+        vals64, _ = cpu_job(raw, fl, dk, geom, reqs, box, "fp64")
         for store, ims in imgs.items():
             rl, mx = [], []
             for (sel, v64), im in zip(vals64, ims):
@@ -587,14 +592,15 @@ def cpu_baseline_and_accuracy(args, geom, raw_dev, flats, darks, reqs, box, upda
                 rl.append(float(np.linalg.norm(got - v64) / np.linalg.norm(v64)))
                 mx.append(float(np.max(np.abs(got - v64))))
             acc[store] = {"rel_l2_vs_fp64": rl, "max_abs_err": mx}
-        acc["sample"] = f"every {stride}th row of each slice's in-box pixels"
+        acc["sample"] = "every in-box pixel of each slice"
     return base, acc
 
 
 # ------------------------------------------------------------------ reference arm
 def run_reference(args, rank, world, local):
     """The reference's CPU implementation of the path (oracle port, all host threads) on
-    the same workload, a bounded sample per step."""
+    the same workload: every step is the whole job, measured; the line reports the
+    median step."""
     if rank != 0:
         return None
     import torch
@@ -605,22 +611,15 @@ def run_reference(args, rank, world, local):
     reqs = slice_requests(box)
     V = WORKLOAD["views"]
     updates = sum(in_box_pixels(box, reqs)) * V
-    view_limit, stride = 96, 16          # per-step sample: 96 views filtered, 1/16 of the rows
-    for _ in range(args.warmup):
-        cpu_job(raw, fl, dk, geom, reqs, box, "ref", stride, view_limit)
-    t_jobs, tms = [], []
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        _, tm = cpu_job(raw, fl, dk, geom, reqs, box, "ref", stride, view_limit)
-        r, t_job = cpu_rate(tm, updates, V)
-        t_jobs.append(t_job)
-        tms.append(tm)
+    runs, tm, _ = cpu_whole_job(raw, fl, dk, geom, reqs, box, reps=args.steps, warmup=args.warmup)
     wall = time.perf_counter() - t0
-    t_job = float(np.mean(t_jobs))
+    t_job = float(np.median(runs))
     value = updates / t_job
-    sample = (f"per step: correction+FDK filter of {view_limit} of {V} views and every {stride}th row of "
-              f"the 3 slices' in-box pixels back-projected from {view_limit} views, on "
-              f"{tms[0]['threads']} host threads; rate extrapolated to the whole job ({t_job:.1f} s)")
+    sample = (f"every step the whole job: correction + FDK filter of all {V} views and every in-box pixel "
+              f"of the 3 slices back-projected from {V} views (C port of the Numba kernel, FP64 "
+              f"accumulation), on {tm['threads']} host threads; median of {len(runs)} steps "
+              f"(min {min(runs):.3f} s, max {max(runs):.3f} s)")
     return {"metric": "voxel-proj updates/s", "value": value, "unit": "updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_job * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -628,10 +627,12 @@ def run_reference(args, rank, world, local):
             "config": {"workload": WORKLOAD_NAME, "views": V, "rows": WORKLOAD["rows"],
                        "cols": WORKLOAD["cols"], "slices": len(reqs), "n": WORKLOAD["n"],
                        "store": "fp32", "accumulate": "f64", "parallelism": "host threads"},
-            "cpu_baseline": {"value": value, "unit": "updates/s", "cores": tms[0]["threads"],
+            "cpu_baseline": {"value": value, "unit": "updates/s", "cores": tm["threads"],
                              "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
+            "timing": {"filter_s_last": tm["t_filter"], "bp_s_last": tm["t_bp"],
+                       "step_s": [round(r, 4) for r in runs]},
             "wall_s": wall}
 
 
@@ -751,6 +752,172 @@ def run_case(args):
     return line
 
 
+def _events_ms(fn, stream, steps, warmup):
+    """Average device time (ms) of fn() over `steps` calls after `warmup`, CUDA events on
+    the stream fn launches on."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _issue_roofline(updates, ms, ops_per_update=FP32_LANE_OPS_PER_UPDATE):
+    ach = updates * ops_per_update / (ms / 1e3) / 1e12
+    peak = NOMINAL_FP32_LANE_OPS / 1e12
+    return {"bound": "fp32-issue", "achieved": ach, "peak": peak, "unit": "T FP32-lane-ops/s",
+            "frac": ach / peak, "ops_per_update": ops_per_update, "updates_per_s": updates / (ms / 1e3),
+            "peak_source": "nominal (148 SMs x 128 FP32 lanes x 1965 MHz); not in MEASURED_PEAKS.json"}
+
+
+def _hbm_roofline(nbytes, ms):
+    pk = _peaks()
+    peak = float(pk.get("hbm_gbs", 6650.0))
+    ach = nbytes / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "algorithmic_bytes": nbytes, "peak_source": "measured" if "hbm_gbs" in pk else "fallback"}
+
+
+KERNEL_CASES = ("bp-plain", "bp-persistent", "grad", "entropy", "preprocess")
+
+
+def run_kernel_case(args):
+    """Kernels outside the headline step, each on the bench scan (600 raw views of
+    486 x 384 ingested into a ring), device-timed with CUDA events:
+    bp-plain       mr_backproject (direct global gathers, FP32 ring), the 3 bench slices in one launch
+    bp-persistent  mr_backproject_persistent (the launch the slice server replays), BF16 ring,
+                   the 3 bench slices, tiles pulled from a device work counter
+    grad           the differentiable back-projector on the FP32 ring over the calibration's two
+                   192^2 slices (axial at z = 0, central x-z) at COR +1.7 px, tilt 0.3 deg:
+                   mr_backproject_matched, mr_project_adjoint (the matched forward projector),
+                   mr_bp_grad_geom (d/dCOR, d/dtilt); each warm-up round launches each once
+    entropy        mr_slice_entropy of the 25 trial 192^2 slices of estimate_cor
+    preprocess     tilt rotation (0.3 deg) then Gaussian (sigma 1 px) of the 600-view block
+                   [384, 600, 486] f32 (mr_rotate_f32, mr_gaussian_axis_f32 x 2); each warm-up
+                   round launches the rotation, then the two Gaussian passes"""
+    import torch
+    from tomography_local_demo_b200 import SliceReconstructor
+    from tomography_local_demo_b200 import _native as N
+    from tomography_local_demo_b200 import preprocess as PP
+    from tomography_local_demo_b200.recon import ctypes_void as cv
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    geom, raw_dev, flats, darks = make_scan(dev)
+    box = geom.volume_box()
+    reqs = slice_requests(box)
+    V = WORKLOAD["views"]
+    idx = np.arange(V)
+    store = {"bp-plain": "fp32", "grad": "fp32"}.get(args.case, "bf16")
+    rec = SliceReconstructor(None, geom, store=store, verbose=False, device=dev, filter="fft")
+    rec.set_flat_dark(as_u16(flats), as_u16(darks))
+    rec.add_raw_projections(idx, raw_dev)
+    torch.cuda.synchronize()
+    steps, warm = args.steps, args.warmup
+    line = {"case": args.case, "steps": steps, "warmup": warm}
+    lib = N.load()
+    if args.case in ("bp-plain", "bp-persistent"):
+        updates = sum(in_box_pixels(box, reqs)) * V
+        if args.case == "bp-plain":
+            rec.bp_kernel = "plain"
+            ms = _events_ms(lambda: rec.reconstruct_planes_tensor(reqs), rec.stream, steps, warm)
+            name = "mr_backproject"
+        else:
+            grids = np.zeros(len(reqs), dtype=N.GRID_DTYPE)
+            off = 0
+            for r, q in enumerate(reqs):
+                grids[r] = rec.plane_grid(q["origin"], q["normal"], q["n"])
+                grids[r]["out_offset"] = off
+                off += q["n"] ** 2
+            grids["n_views"], grids["scale"] = V, np.pi / V
+            tiles = N.plan_tiles(grids, rec._band_axis)
+            recs = torch.from_numpy(np.concatenate([grids.view(np.uint8), tiles.view(np.uint8)])).to(dev)
+            nt = torch.tensor([len(tiles)], dtype=torch.int64, device=dev)
+            counter = torch.zeros(1, dtype=torch.int32, device=dev)
+            status = torch.zeros(1, dtype=torch.int32, device=dev)
+            out = torch.empty(off, dtype=torch.float32, device=dev)
+            st = torch.cuda.current_stream(dev)
+
+            def launch():
+                N.check(lib.mr_backproject_persistent(
+                    rec._ring_c, cv(rec._views_dev.data_ptr()), cv(recs.data_ptr()),
+                    cv(recs.data_ptr() + grids.nbytes), cv(nt.data_ptr()), len(tiles), cv(counter.data_ptr()),
+                    cv(out.data_ptr()), cv(status.data_ptr()), cv(st.cuda_stream)), "mr_backproject_persistent")
+            ms = _events_ms(launch, st, steps, warm)
+            assert int(status.item()) == 0, "a bounded device-side wait gave up"
+            name = "mr_backproject_persistent"
+        line.update(kernel=name, workload="3 oblique 512^2 slices x 600 views, " + store + " ring",
+                    ms=ms, updates=updates, roofline=_issue_roofline(updates, ms))
+    elif args.case == "grad":
+        creqs = [dict(origin=(0.0, 0.0, 0.0), normal=(0.0, 0.0, 1.0), n=192),
+                 dict(origin=(0.0, 0.0, 0.0), normal=(0.0, 1.0, 0.0), n=192)]
+        op = rec.bp_operator(creqs)
+        q = rec._ring
+        shift, tilt = 1.7, float(np.deg2rad(0.3))
+        st = torch.cuda.current_stream(dev)
+        f = op.forward(q, shift, tilt)
+        updates = int((f != 0).sum()) * V
+        y = torch.randn(op.n_out, generator=torch.Generator(device=dev).manual_seed(3), device=dev)
+        fns = [lambda: op.forward(q, shift, tilt), lambda: op.adjoint(y, shift, tilt, tuple(q.shape)),
+               lambda: op.grad_geometry(q, y, shift, tilt)]
+        for _ in range(warm):              # one launch of each kernel per warm-up round
+            for fn in fns:
+                fn()
+        ms_f, ms_a, ms_g = (_events_ms(fn, st, steps, 0) for fn in fns)
+        line.update(workload="2 calibration slices 192^2 (axial z=0, x-z) x 600 views, fp32 ring, "
+                             "COR +1.7 px, tilt 0.3 deg", updates=updates,
+                    kernels={"mr_backproject_matched": {"ms": ms_f, "roofline": _issue_roofline(updates, ms_f)},
+                             "mr_project_adjoint": {"ms": ms_a, "roofline": _issue_roofline(updates, ms_a),
+                                                    "atomics_per_s": 4 * updates / (ms_a / 1e3),
+                                                    "note": "time includes zeroing the 448 MB gradient ring"},
+                             "mr_bp_grad_geom": {"ms": ms_g, "roofline": _issue_roofline(updates, ms_g)}})
+    elif args.case == "entropy":
+        shifts = np.arange(-3.0, 3.01, 0.25)
+        creqs = [dict(origin=(0.0, 0.0, 0.0), normal=(0.0, 0.0, 1.0), n=192, cor_shift=float(s)) for s in shifts]
+        imgs, _ = rec._planes(creqs)
+        torch.cuda.synchronize()
+        scores = torch.empty(len(creqs), dtype=torch.float64, device=dev)
+        st = torch.cuda.current_stream(dev)
+        n2 = 192 * 192
+
+        def launch():
+            N.check(lib.mr_slice_entropy(cv(imgs.data_ptr()), len(creqs), n2, n2, 128, cv(scores.data_ptr()),
+                                         cv(st.cuda_stream)), "mr_slice_entropy")
+        ms = _events_ms(launch, st, steps, warm)
+        nbytes = 2 * len(creqs) * n2 * 4           # two passes over the pixels (range, then bins)
+        line.update(kernel="mr_slice_entropy", workload="25 trial axial slices 192^2, 128 bins", ms=ms,
+                    roofline=_hbm_roofline(nbytes, ms),
+                    note="one CTA per trial slice: 25 CTAs on 148 SMs, 3.7 MB that stays in L2")
+    elif args.case == "preprocess":
+        R, C = WORKLOAD["rows"], WORKLOAD["cols"]
+        x = torch.rand((R, V, C), generator=torch.Generator(device=dev).manual_seed(1), device=dev)
+        st = torch.cuda.current_stream(dev)
+        fns = [lambda: PP._rotate_dev(x, -0.3), lambda: PP._gaussian_dev(x, 1.0)]
+        for _ in range(warm):              # rotation, then the two Gaussian passes, per round
+            for fn in fns:
+                fn()
+        ms_r, ms_g = (_events_ms(fn, st, steps, 0) for fn in fns)
+        px = R * V * C
+        line.update(workload="block [384, 600, 486] f32 (448 MB)",
+                    kernels={"mr_rotate_f32": {"ms": ms_r, "roofline": _hbm_roofline(8 * px, ms_r)},
+                             "mr_gaussian_axis_f32 (rows, then cols)": {"ms": ms_g,
+                                                                        "roofline": _hbm_roofline(16 * px, ms_g)}})
+    return line
+
+
 def run_wire_case(args):
     """The `wire` case of run_case: host wall clock per step through net.Server."""
     import threading
@@ -803,12 +970,16 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the live-scan serving simulation")
     ap.add_argument("--filter", choices=("fft", "tc", "tc-bf16"), default="tc",
                     help="row filter: shared-memory FFT or tensor-core Toeplitz GEMM (split FP16 / BF16)")
-    ap.add_argument("--case", choices=("otsu", "surface", "correct", "ingest-full", "parker", "wire"), default=None,
+    ap.add_argument("--case", choices=("otsu", "surface", "correct", "ingest-full", "parker", "wire") + KERNEL_CASES,
+                    default=None,
                     help="time one other kernel family alone instead of the headline step")
     ap.add_argument("--case-views", type=int, default=0, help="views of the correct / ingest-full case")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.case in KERNEL_CASES:
+        print(json.dumps(run_kernel_case(args)), flush=True)
+        return
     if args.case is not None:
         print(json.dumps(run_case(args)), flush=True)
         return
