@@ -71,3 +71,39 @@ def test_write_stl(tmp_path):
     np.testing.assert_allclose(n, [0, 0, -1], atol=1e-7)
     with pytest.raises(SystemExit):
         M.save_mesh({"points": P, "faces": F}, str(tmp_path / "m.ply"))
+
+
+def edge_crossing_vertices(vol, iso, origin, h):
+    """The vertex set of an iso-contour as every marching-cubes variant emits it, the
+    reference's contour included (model.py:54 VTK flying edges, model.py:72-75 scikit-image
+    marching_cubes): one vertex on each grid edge whose end values lie on opposite sides of
+    iso, at the linear interpolation point p0 + (iso - f0) / (f1 - f0) (p1 - p0), in float64.
+    Written from that definition alone (no case table), so it pins the vertices of the
+    surface to the reference's independently of the triangulation of ambiguous cells."""
+    vol = np.asarray(vol, np.float64)
+    out = []
+    for axis in range(3):
+        n = vol.shape[axis]
+        f0 = np.take(vol, np.arange(n - 1), axis=axis)
+        f1 = np.take(vol, np.arange(1, n), axis=axis)
+        cross = (f0 < iso) != (f1 < iso)
+        idx = np.argwhere(cross).astype(np.float64)
+        t = (iso - f0[cross]) / (f1[cross] - f0[cross])
+        idx[:, axis] += t
+        out.append(np.asarray(origin, np.float64) + h * idx)
+    return sorted_rows(np.concatenate(out))
+
+
+def sorted_rows(P):
+    P = np.asarray(P, np.float64)
+    return P[np.lexsort(P.T[::-1])]
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_oracle_vertices_are_the_contour_edge_crossings(seed):
+    rng = np.random.default_rng(seed)
+    vol = rng.normal(size=(13, 17, 11)).astype(np.float32)
+    P, F = om.marching_cubes(vol, 0.1, (1.0, -2.0, 0.5), 0.7)
+    want = edge_crossing_vertices(vol, 0.1, (1.0, -2.0, 0.5), 0.7)
+    assert len(P) == len(want)
+    np.testing.assert_allclose(sorted_rows(P), want, rtol=0, atol=1e-5)

@@ -45,6 +45,20 @@ def test_marching_cubes_equals_oracle(cuda, name, vol, iso, origin, h):
     np.testing.assert_array_equal(F.cpu().numpy(), want_F)
 
 
+@pytest.mark.parametrize("name,vol,iso,origin,h", list(_cases()), ids=[c[0] for c in _cases()])
+def test_device_vertices_are_the_contour_edge_crossings(cuda, name, vol, iso, origin, h):
+    """The device surface has exactly the vertex set that any marching-cubes contour of
+    the reference (VTK flying edges or scikit-image) has: one vertex per crossed grid
+    edge at the linear interpolation point (restated in test_surface.py from that
+    definition alone), to FP32 rounding."""
+    from test_surface import edge_crossing_vertices, sorted_rows
+    P, _ = M.marching_cubes(torch.from_numpy(vol).cuda(), iso, origin, h)
+    want = edge_crossing_vertices(vol, iso, origin, h)
+    assert len(P) == len(want)
+    scale = max(1.0, float(np.abs(want).max()))
+    np.testing.assert_allclose(sorted_rows(P.cpu().numpy()), want, rtol=0, atol=2e-6 * scale)
+
+
 def test_sphere_surface_closed_with_the_right_area(cuda):
     P, F = M.marching_cubes(_sphere(96, 40.0), 0.0)
     P, F = P.cpu().numpy().astype(np.float64), F.cpu().numpy()

@@ -1497,12 +1497,12 @@ class SliceReconstructor:
                 J = J + soft_neg_entropy(f[o:o + sz].double(), lo, hi)
                 o += sz
             if not grad:
-                return float(J), None
+                return float(J.detach()), None
             J.backward()
             g = xs.grad.clone()
             if not fit_tilt:
                 g[1] = 0.0
-            return float(J), g
+            return float(J.detach()), g
 
         J, g = score(x)
         step = 0.5
