@@ -32,11 +32,14 @@ namespace mr {
 constexpr int ST_TI = 32, ST_TJ = 32;        // tile (samples) - same tiling as bp.cu
 constexpr int ST_CONSUMERS = 8;               // consumer warps (one 32 x 32 tile)
 constexpr int ST_THREADS = 32 * (ST_CONSUMERS + 1);   // + one producer warp
-constexpr int ST_PPT = 4;                     // samples per consumer thread (i, i+4, i+8, i+12)
+constexpr int ST_PPT = 4;                     // samples per consumer thread (rows i, i+2, i+4, i+6)
+constexpr int ST_DI = 2;                      // row step between a thread's samples
 constexpr int ST_BOX_H = 8;                   // rows per TMA box
 constexpr int ST_CLUSTER = 4;                 // CTAs per tile, each a quarter of the views
 constexpr float MAGIC = 12582912.0f;          // 1.5 * 2^23
 constexpr int MAGIC_BITS = 0x4B400000;
+#define kMagic2 make_float2(MAGIC, MAGIC)
+#define kNeg2 make_float2(-1.f, -1.f)
 
 template <typename T> struct StageGeom;
 // Row widths (elements) are 16-byte multiples whose word pitch shifts successive rows
@@ -49,8 +52,16 @@ template <> struct StageGeom<float> { static constexpr int W = 84, ALIGN = 4, ST
 
 enum : int { MODE_STAGED = 0, MODE_GLOBAL = 1, MODE_SKIP = 2 };
 
+// What the consumer warps read per (tile, view): the local affine maps of the projective
+// numerators u, v and denominator w, (value at the tile origin, d/di, d/dj), in stage-local
+// coordinates, packed into three 16-byte words:
+//   a = (u0, u_i, u_j, v0), b = (v_i, v_j, w0, w_i), c = (w_j, qscale, max tap offset, mode)
+struct __align__(16) ViewRec {
+    float4 a, b, c;
+};
+// The producer's copy adds the TMA box origin and count.
 struct __align__(16) ViewMeta {
-    float4 cu, cv, cw;       // (value at tile origin, d/di, d/dj, qscale|-|-) in local coords
+    ViewRec rec;
     int x0, r0, nbox, mode;
 };
 
@@ -217,15 +228,18 @@ __device__ __forceinline__ ViewMeta view_meta(const mr_view& V, const mr_grid& g
             if ((int)floorf(cmax) + 3 - x0 <= W && nbox <= StageGeom<T>::MAXB) mode = MODE_STAGED;
         }
     }
+    float3 cu = au, cv = av;
     if (mode == MODE_STAGED) {
         const float fx0 = (float)x0, fr0 = (float)r0;
-        m.cu = make_float4(fmaf(-fx0, aw.x, au.x), fmaf(-fx0, aw.y, au.y), fmaf(-fx0, aw.z, au.z), V.qscale);
-        m.cv = make_float4(fmaf(-fr0, aw.x, av.x), fmaf(-fr0, aw.y, av.y), fmaf(-fr0, aw.z, av.z), 0.f);
-    } else {
-        m.cu = make_float4(au.x, au.y, au.z, V.qscale);
-        m.cv = make_float4(av.x, av.y, av.z, 0.f);
+        cu = make_float3(fmaf(-fx0, aw.x, au.x), fmaf(-fx0, aw.y, au.y), fmaf(-fx0, aw.z, au.z));
+        cv = make_float3(fmaf(-fr0, aw.x, av.x), fmaf(-fr0, aw.y, av.y), fmaf(-fr0, aw.z, av.z));
     }
-    m.cw = make_float4(aw.x, aw.y, aw.z, 0.f);
+    // largest byte offset of a tap pair's left tap inside the staged boxes
+    constexpr int ESZ = (int)sizeof(T);
+    const uint32_t maxoff = mode == MODE_STAGED ? (uint32_t)(nbox * W * ST_BOX_H * ESZ - (W + 1) * ESZ - ESZ) : 0u;
+    m.rec.a = make_float4(cu.x, cu.y, cu.z, cv.x);
+    m.rec.b = make_float4(cv.y, cv.z, aw.x, aw.y);
+    m.rec.c = make_float4(aw.z, V.qscale, __uint_as_float(maxoff), __int_as_float(mode));
     m.x0 = x0; m.r0 = r0; m.nbox = nbox; m.mode = mode;
     return m;
 }
@@ -237,8 +251,10 @@ __device__ __forceinline__ ViewMeta view_meta(const mr_view& V, const mr_grid& g
 // A thread-block cluster of ST_CLUSTER CTAs shares one tile: CTA rank r back-projects the
 // r-th quarter of the views and rank 0 sums the partials from the others' shared memory
 // (DSMEM) in rank order - deterministic, no atomics, no scratch - and writes the tile.
+// Three CTAs fit an SM (shared memory); the launch bound says so, or ptxas aims at four and
+// spills the FP32 variant to fit its registers.
 template <int KIND, typename T>
-__global__ void __launch_bounds__(ST_THREADS)
+__global__ void __launch_bounds__(ST_THREADS, 3)
 bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__ ring, int R, int C,
                  int pitch, long long slot_stride, int n_slots, const mr_view* __restrict__ views,
                  const mr_grid* __restrict__ grids, const mr_tile* __restrict__ tiles,
@@ -257,8 +273,8 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
     // allocates 128 spare bytes), whatever static shared memory precedes it.
     unsigned char* stages = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~static_cast<uintptr_t>(127));
-    ViewMeta* meta_ring = reinterpret_cast<ViewMeta*>(stages + S * STAGE_BYTES);   // S
-    ViewMeta* meta_new = meta_ring + S;                                              // 32
+    ViewRec* meta_ring = reinterpret_cast<ViewRec*>(stages + S * STAGE_BYTES);     // S
+    ViewMeta* meta_new = reinterpret_cast<ViewMeta*>(meta_ring + S);                // 32
     uint64_t* full = reinterpret_cast<uint64_t*>(meta_new + 32);                    // S
     uint64_t* empty = full + S;                                                      // S
     float4* partial = reinterpret_cast<float4*>(empty + S);                          // 256 (cluster sum)
@@ -315,13 +331,18 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
         const float ox = g.origin[0] + t.i0 * g.step_i[0] + t.j0 * g.step_j[0] + t.k * g.step_k[0];
         const float oy = g.origin[1] + t.i0 * g.step_i[1] + t.j0 * g.step_j[1] + t.k * g.step_k[1];
         const float oz = g.origin[2] + t.i0 * g.step_i[2] + t.j0 * g.step_j[2] + t.k * g.step_k[2];
-        const int tx = ((warp & 3) << 3) | (lane & 7);
-        const int ty = ((warp >> 2) << 4) | (lane >> 3);
+        // warp w covers columns 16 (w & 1) .. + 15 and rows 8 (w >> 1) .. + 7 of the tile; its
+        // p-th sample step is a 16 x 2 patch (rows ty + 2p). The patch shape keeps the 32
+        // lanes' bilinear taps on distinct shared-memory banks for most plane orientations
+        // (1.10 wavefronts per 16-bit tap load on the bench slices, 1.35 for 8 x 4 patches)
+        // and makes each half-warp's output a 64-byte row segment.
+        const int tx = ((warp & 1) << 4) | (lane & 15);
+        const int ty = ((warp >> 1) << 3) | (lane >> 4);
         bool inside[ST_PPT];
         bool any = false;
 #pragma unroll
         for (int p = 0; p < ST_PPT; ++p) {
-            const int i = t.i0 + ty + 4 * p, j = t.j0 + tx;
+            const int i = t.i0 + ty + ST_DI * p, j = t.j0 + tx;
             bool ok = !producer && i < g.n_i && j < g.n_j;
             if (ok && (g.flags & MR_GRID_MASK_BOX)) ok = in_box_fp64_t(g, i, j);
             inside[p] = ok;
@@ -350,7 +371,7 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                         const uint32_t u = ua / S;
                         if (u > 0) mbar_wait(&empty[s], (u - 1) & 1u, status);
                         const ViewMeta m = meta_new[l];
-                        meta_ring[s] = m;
+                        meta_ring[s] = m.rec;
                         if (m.mode == MODE_STAGED) {
                             mbar_arrive_tx(&full[s], (uint32_t)(m.nbox * BOX_BYTES));
                             unsigned char* dst = stages + s * STAGE_BYTES;
@@ -365,91 +386,115 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
             }
         }
 
-        float acc[ST_PPT];
+        // sample p sits in pair p / 2, lane p % 2 (pairs of rows i and i + ST_DI)
+        float2 acc2[ST_PPT / 2];
+        float2 fi2[ST_PPT / 2];
 #pragma unroll
-        for (int p = 0; p < ST_PPT; ++p) acc[p] = 0.f;
+        for (int h = 0; h < ST_PPT / 2; ++h) {
+            acc2[h] = make_float2(0.f, 0.f);
+            fi2[h] = make_float2((float)(ty + 2 * ST_DI * h), (float)(ty + 2 * ST_DI * h + ST_DI));
+        }
         if (!producer && tile_live) {
             const float fj = (float)tx;
+            int s = (int)(used % S);                    // stage of view 0 of this tile
+            uint32_t phase = (used / S) & 1u;           // and the parity of its fill
             for (int v = 0; v < nv; ++v) {
-                const uint32_t ua = used + (uint32_t)v;
-                const int s = (int)(ua % S);
-                mbar_wait(&full[s], (ua / S) & 1u, status);
-                const ViewMeta m = meta_ring[s];
-                const float bu = fmaf(fj, m.cu.z, m.cu.x);
-                const float bv = fmaf(fj, m.cv.z, m.cv.x);
-                const float bw = fmaf(fj, m.cw.z, m.cw.x);
-                if (m.mode == MODE_STAGED) {
+                mbar_wait(&full[s], phase, status);
+                const ViewRec m = meta_ring[s];
+                const int mode = __float_as_int(m.c.w);
+                const float bu = fmaf(fj, m.a.z, m.a.x);
+                const float bv = fmaf(fj, m.b.y, m.a.w);
+                const float bw = fmaf(fj, m.c.x, m.b.z);
+                if (mode == MODE_STAGED) {
                     const uint32_t base = smem_u32(stages + s * STAGE_BYTES);
-                    const uint32_t maxoff = (uint32_t)(m.nbox * BOX_BYTES - (W + 1) * ESZ - ESZ);
+                    const uint32_t maxoff = __float_as_uint(m.c.z);
                     // byte offset = (bits_r - MAGIC_BITS) * W*ESZ + (bits_c - MAGIC_BITS) * ESZ
                     const uint32_t kofs = (uint32_t)MAGIC_BITS * (uint32_t)(W * ESZ + ESZ);
+                    // Two samples (rows i and i + 2) per packed f32x2 instruction: every
+                    // component is the scalar FMA / add / multiply it replaces, so the result
+                    // is the same bit for bit; only the issue slots halve.
+                    const float2 cuy = make_float2(m.a.y, m.a.y), cvy = make_float2(m.b.x, m.b.x);
+                    const float2 cwy = make_float2(m.b.w, m.b.w);
+                    const float2 bu2 = make_float2(bu, bu), bv2 = make_float2(bv, bv), bw2 = make_float2(bw, bw);
 #pragma unroll
-                    for (int p = 0; p < ST_PPT; ++p) {
-                        if (!wlive[p]) continue;
-                        const float fi = (float)(ty + 4 * p);
-                        const float nu = fmaf(fi, m.cu.y, bu);
-                        const float nvv = fmaf(fi, m.cv.y, bv);
-                        float r = 1.f, yc, yr, fc, fr;
+                    for (int h = 0; h < ST_PPT / 2; ++h) {
+                        if (!(wlive[2 * h] | wlive[2 * h + 1])) continue;
+                        const float2 nu = __ffma2_rn(fi2[h], cuy, bu2);
+                        const float2 nv2 = __ffma2_rn(fi2[h], cvy, bv2);
+                        float2 r = make_float2(1.f, 1.f), yc, yr, fc, fr;
                         if (KIND == MR_CONE) {
-                            r = rcp_approx(fmaf(fi, m.cw.y, bw));
-                            yc = __fmaf_rd(nu, r, MAGIC);
-                            yr = __fmaf_rd(nvv, r, MAGIC);
-                            fc = fmaf(nu, r, MAGIC - yc);
-                            fr = fmaf(nvv, r, MAGIC - yr);
+                            const float2 w = __ffma2_rn(fi2[h], cwy, bw2);
+                            r = make_float2(rcp_approx(w.x), rcp_approx(w.y));
+                            yc = __ffma2_rd(nu, r, kMagic2);
+                            yr = __ffma2_rd(nv2, r, kMagic2);
+                            // MAGIC - y is exact; fma(y, -1, MAGIC) is that subtraction
+                            fc = __ffma2_rn(nu, r, __ffma2_rn(yc, kNeg2, kMagic2));
+                            fr = __ffma2_rn(nv2, r, __ffma2_rn(yr, kNeg2, kMagic2));
                         } else {
-                            yc = __fadd_rd(nu, MAGIC);
-                            yr = __fadd_rd(nvv, MAGIC);
-                            fc = nu + (MAGIC - yc);
-                            fr = nvv + (MAGIC - yr);
+                            yc = __fadd2_rd(nu, kMagic2);
+                            yr = __fadd2_rd(nv2, kMagic2);
+                            fc = __fadd2_rn(nu, __ffma2_rn(yc, kNeg2, kMagic2));
+                            fr = __fadd2_rn(nv2, __ffma2_rn(yr, kNeg2, kMagic2));
                         }
-                        uint32_t off = (uint32_t)__float_as_int(yr) * (uint32_t)(W * ESZ) +
-                                       (uint32_t)__float_as_int(yc) * (uint32_t)ESZ - kofs;
-                        off = min(off, maxoff);
-                        const uint32_t a = base + off;
-                        float ta, tb;
+                        uint32_t a[2];
+                        a[0] = base + min((uint32_t)__float_as_int(yr.x) * (uint32_t)(W * ESZ) +
+                                              (uint32_t)__float_as_int(yc.x) * (uint32_t)ESZ - kofs, maxoff);
+                        a[1] = base + min((uint32_t)__float_as_int(yr.y) * (uint32_t)(W * ESZ) +
+                                              (uint32_t)__float_as_int(yc.y) * (uint32_t)ESZ - kofs, maxoff);
+                        float2 q00, q10, d0, d1;
                         if constexpr (sizeof(T) == 2) {
                             // the right taps stay 16-bit: one mixed-precision subtraction each
-                            // (16-bit values widen exactly, so it is the FP32 difference) instead
-                            // of a widening and an FP32 subtraction
-                            const unsigned short u01 = lds_u16(a + ESZ), u11 = lds_u16(a + W * ESZ + ESZ);
-                            const float q00 = lds_elem<T>(a);
-                            const float q10 = lds_elem<T>(a + W * ESZ);
-                            ta = fmaf(fc, sub16_f32<T>(u01, q00), q00);
-                            tb = fmaf(fc, sub16_f32<T>(u11, q10), q10);
+                            // (16-bit values widen exactly, so it is the FP32 difference)
+                            q00 = make_float2(lds_elem<T>(a[0]), lds_elem<T>(a[1]));
+                            q10 = make_float2(lds_elem<T>(a[0] + W * ESZ), lds_elem<T>(a[1] + W * ESZ));
+                            d0 = make_float2(sub16_f32<T>(lds_u16(a[0] + ESZ), q00.x),
+                                             sub16_f32<T>(lds_u16(a[1] + ESZ), q00.y));
+                            d1 = make_float2(sub16_f32<T>(lds_u16(a[0] + W * ESZ + ESZ), q10.x),
+                                             sub16_f32<T>(lds_u16(a[1] + W * ESZ + ESZ), q10.y));
                         } else {
-                            const float q00 = lds_elem<T>(a);
-                            const float q01 = lds_elem<T>(a + ESZ);
-                            const float q10 = lds_elem<T>(a + W * ESZ);
-                            const float q11 = lds_elem<T>(a + W * ESZ + ESZ);
-                            ta = fmaf(fc, q01 - q00, q00);
-                            tb = fmaf(fc, q11 - q10, q10);
+                            q00 = make_float2(lds_elem<T>(a[0]), lds_elem<T>(a[1]));
+                            q10 = make_float2(lds_elem<T>(a[0] + W * ESZ), lds_elem<T>(a[1] + W * ESZ));
+                            const float2 q01 = make_float2(lds_elem<T>(a[0] + ESZ), lds_elem<T>(a[1] + ESZ));
+                            const float2 q11 = make_float2(lds_elem<T>(a[0] + W * ESZ + ESZ),
+                                                           lds_elem<T>(a[1] + W * ESZ + ESZ));
+                            d0 = __ffma2_rn(q00, kNeg2, q01);          // q01 - q00
+                            d1 = __ffma2_rn(q10, kNeg2, q11);          // q11 - q10
                         }
-                        const float val = fmaf(fr, tb - ta, ta);
-                        acc[p] = fmaf(KIND == MR_CONE ? r * r : m.cu.w, val, acc[p]);
+                        const float2 ta = __ffma2_rn(fc, d0, q00);
+                        const float2 tb = __ffma2_rn(fc, d1, q10);
+                        const float2 val = __ffma2_rn(fr, __ffma2_rn(ta, kNeg2, tb), ta);
+                        const float2 wgt = KIND == MR_CONE ? __fmul2_rn(r, r) : make_float2(m.c.y, m.c.y);
+                        acc2[h] = __ffma2_rn(wgt, val, acc2[h]);
                     }
-                } else if (m.mode == MODE_GLOBAL) {
+                } else if (mode == MODE_GLOBAL) {
                     const T* q = ring + (long long)(v_begin + v) * slot_stride;
 #pragma unroll
                     for (int p = 0; p < ST_PPT; ++p) {
                         if (!wlive[p]) continue;
-                        const float fi = (float)(ty + 4 * p);
-                        const float nu = fmaf(fi, m.cu.y, bu);
-                        const float nvv = fmaf(fi, m.cv.y, bv);
+                        const float fi = (float)(ty + ST_DI * p);
+                        const float nu = fmaf(fi, m.a.y, bu);
+                        const float nvv = fmaf(fi, m.b.x, bv);
+                        float& ap = (p & 1) ? acc2[p >> 1].y : acc2[p >> 1].x;
                         if (KIND == MR_CONE) {
-                            const float r = rcp_approx(fmaf(fi, m.cw.y, bw));
-                            acc[p] = fmaf(r * r, bilerp_global(q, R, C, pitch, nvv * r, nu * r), acc[p]);
+                            const float r = rcp_approx(fmaf(fi, m.b.w, bw));
+                            ap = fmaf(r * r, bilerp_global(q, R, C, pitch, nvv * r, nu * r), ap);
                         } else {
-                            acc[p] = fmaf(m.cu.w, bilerp_global(q, R, C, pitch, nvv, nu), acc[p]);
+                            ap = fmaf(m.c.y, bilerp_global(q, R, C, pitch, nvv, nu), ap);
                         }
                     }
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty[s]);      // this warp is done with stage s
+                if (++s == S) {
+                    s = 0;
+                    phase ^= 1u;
+                }
             }
         }
         if (tile_live) used += (uint32_t)nv;
 
         // ---- cluster reduction of the view-quarter partial sums (rank order), rank 0 writes
+        float acc[ST_PPT] = {acc2[0].x, acc2[0].y, acc2[1].x, acc2[1].y};
         if (csize > 1) {
             if (!producer) partial[tid] = make_float4(acc[0], acc[1], acc[2], acc[3]);
             cluster.sync();
@@ -463,7 +508,7 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
         if (crank == 0 && !producer) {
 #pragma unroll
             for (int p = 0; p < ST_PPT; ++p) {
-                const int i = t.i0 + ty + 4 * p, j = t.j0 + tx;
+                const int i = t.i0 + ty + ST_DI * p, j = t.j0 + tx;
                 if (i < g.n_i && j < g.n_j) {
                     const long long o = g.out_offset + (long long)i * g.out_stride_i +
                                         (long long)j * g.out_stride_j + (long long)t.k * g.out_stride_k;
@@ -517,7 +562,7 @@ static int launch_staged(const mr_ring* ring, const mr_view* views, const mr_gri
     if (rc != MR_OK) return rc;
     constexpr int S = StageGeom<T>::STAGES;
     const size_t smem = (size_t)S * StageGeom<T>::W * ST_BOX_H * StageGeom<T>::MAXB * sizeof(T) +
-                        (S + 32) * sizeof(ViewMeta) + 2 * S * sizeof(uint64_t) +
+                        S * sizeof(ViewRec) + 32 * sizeof(ViewMeta) + 2 * S * sizeof(uint64_t) +
                         ST_CONSUMERS * 32 * sizeof(float4) + 128;
     auto kern = bp_staged_kernel<KIND, T>;
     MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
