@@ -70,7 +70,9 @@ __device__ __forceinline__ float2 twiddle(float2 x) {
         return make_float2(x.y, -x.x);
     } else {
         constexpr float c = kTw<R>.re[K], s = kTw<R>.im[K];
-        return make_float2(fmaf(x.x, c, -x.y * s), fmaf(x.x, s, x.y * c));
+        // (x.x c - x.y s, x.x s + x.y c) as two packed operations (same roundings)
+        return __ffma2_rn(make_float2(x.x, x.x), make_float2(c, s),
+                          __fmul2_rn(make_float2(x.y, x.y), make_float2(-s, c)));
     }
 }
 
@@ -439,7 +441,7 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A) {
 #pragma unroll
                 for (int q = 0; q < 32; ++q) {
                     const float h = __ldg(A.H + j + G * q) * g;
-                    x[q] = make_float2(x[q].x * h, -x[q].y * h);
+                    x[q] = __fmul2_rn(x[q], make_float2(h, -h));
                 }
             }
         }

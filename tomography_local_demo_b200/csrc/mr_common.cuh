@@ -53,11 +53,15 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return r;
 }
 
+// Complex arithmetic on (re, im) pairs with the packed f32x2 instructions of sm_100: each
+// component is exactly the scalar operation it replaces (a - b is fma(b, -1, a), one
+// rounding of the exact difference), so results are unchanged and the issue slots halve.
+//   a b = (a.x b.x - a.y b.y, a.x b.y + a.y b.x) = a.x (b.x, b.y) + a.y (-b.y, b.x)
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+    return __ffma2_rn(make_float2(a.x, a.x), b, __fmul2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x)));
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 
 // Per-view projective map with the grid's COR shift and detector tilt applied:
 //   no tilt: pu' = pu + shift pw,  pv' = pv + shift uv pw                 (recon.py:420)
