@@ -131,3 +131,15 @@ def test_preprocess_matches_reference(cuda, op):
     rot = P.rotate_projections(g["point"], 90.0)
     r, c = np.unravel_index(np.argmax(rot[:, 0, :]), (41, 41))
     assert (r, c) in ((10, 20), (30, 20))
+
+
+@pytest.mark.parametrize("shape,sigma", [((96, 7, 150), 1.0), ((37, 5, 300), 0.8), ((130, 3, 61), 2.5),
+                                         ((384, 2, 486), 1.0)])
+def test_gaussian_blur_against_oracle_at_size(cuda, shape, sigma):
+    """The staged shared-memory Gaussian (lines that are not a multiple of the block's line
+    count, lengths that are not a multiple of its output span, taps reaching half the
+    padded length at small sigma) against the oracle's FFT restatement of
+    preprocess.py:8-28."""
+    rng = np.random.default_rng(int(sigma * 10) + shape[0])
+    block = rng.normal(1.0, 0.3, shape).astype(np.float32)
+    close(P.gaussian_blur(block, sigma), of.gaussian_blur(block, sigma), 1e-5)

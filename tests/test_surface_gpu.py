@@ -51,12 +51,11 @@ def test_device_vertices_are_the_contour_edge_crossings(cuda, name, vol, iso, or
     the reference (VTK flying edges or scikit-image) has: one vertex per crossed grid
     edge at the linear interpolation point (restated in test_surface.py from that
     definition alone), to FP32 rounding."""
-    from test_surface import edge_crossing_vertices, sorted_rows
+    from test_surface import assert_same_vertex_set, edge_crossing_vertices
     P, _ = M.marching_cubes(torch.from_numpy(vol).cuda(), iso, origin, h)
     want = edge_crossing_vertices(vol, iso, origin, h)
-    assert len(P) == len(want)
     scale = max(1.0, float(np.abs(want).max()))
-    np.testing.assert_allclose(sorted_rows(P.cpu().numpy()), want, rtol=0, atol=2e-6 * scale)
+    assert_same_vertex_set(P.cpu().numpy(), want, 4e-6 * scale)
 
 
 def test_sphere_surface_closed_with_the_right_area(cuda):

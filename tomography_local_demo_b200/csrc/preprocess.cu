@@ -64,6 +64,93 @@ __global__ void gauss_axis_kernel(const float* __restrict__ in, float* __restric
     out[r * srow + (long long)a * C + c] = acc;
 }
 
+// The same axis convolution organised for the SM. For small sigma the taps reach about half
+// the padded length (the spectrum is cut at Nyquist), so a direct loop costs ~n/2 taps per
+// output. A block takes L lines (rows along axis 2, columns along axis 0) and TO outputs of
+// each: it stages the stretch of the edge-padded, periodically extended line those outputs
+// read - padded positions i0 + pad - K .. i0 + TO - 1 + pad + K - into shared memory once,
+// then every thread slides a window of 8 consecutive outputs of one line over the taps: one
+// shared load and 8 FMAs per tap. Each output sums its taps m = -K .. K in the same order
+// and with the same FMAs as gauss_axis_kernel, so the results are identical.
+constexpr int GS_THREADS = 256;
+constexpr int GS_RUN = 8;                       // consecutive outputs per thread
+
+template <int L>
+__global__ void __launch_bounds__(GS_THREADS)
+gauss_lines_kernel(const float* __restrict__ in, float* __restrict__ out, int R, int A, int C, int axis,
+                   int pad, const float* __restrict__ g, int K, int TO) {
+    extern __shared__ float gsm[];
+    constexpr int LP = L + 1;                   // padded line stride: conflict-free stores
+    const int T = TO + 2 * K;                   // staged padded positions per line
+    float* ext = gsm;                           // [T][LP]
+    float* taps = gsm + (size_t)T * LP;         // [K + 1]
+    const long long srow = (long long)A * C;
+    const int n = axis == 0 ? R : C;
+    const int Np = n + 2 * pad;
+    const long long n_lines = axis == 0 ? (long long)A * C : (long long)R * A;
+    const long long line0 = (long long)blockIdx.x * L;
+    const int i0 = blockIdx.y * TO;
+    const long long step = axis == 0 ? srow : 1;
+    auto line_base = [&](long long line) -> long long {
+        if (axis == 0) return line;                                     // a * C + c
+        const long long r = line / A, a = line - r * A;
+        return r * srow + a * C;
+    };
+    for (int m = threadIdx.x; m <= K; m += GS_THREADS) taps[m] = __ldg(g + m);
+    const int nl = (int)min((long long)L, n_lines - line0);
+    for (int e = threadIdx.x; e < L * T; e += GS_THREADS) {
+        int l, t;
+        if (axis == 0) { l = e % L; t = e / L; }                        // neighbouring columns
+        else { l = e / T; t = e - (e / T) * T; }                        // along one row
+        float v = 0.f;
+        if (l < nl) {
+            int u = i0 + pad - K + t;                                   // padded position
+            u %= Np;
+            if (u < 0) u += Np;                                         // circular
+            int src = u - pad;                                          // edge padding
+            src = src < 0 ? 0 : (src >= n ? n - 1 : src);
+            v = __ldg(in + line_base(line0 + l) + src * step);
+        }
+        ext[t * LP + l] = v;
+    }
+    __syncthreads();
+    const int groups = (TO + GS_RUN - 1) / GS_RUN;
+    for (int task = threadIdx.x; task < L * groups; task += GS_THREADS) {
+        const int l = task % L, q = task / L;
+        const int o0 = q * GS_RUN;                                      // first output (block-local)
+        if (l >= nl || i0 + o0 >= n) continue;
+        float acc[GS_RUN];
+        float win[GS_RUN];
+#pragma unroll
+        for (int j = 0; j < GS_RUN; ++j) {
+            acc[j] = 0.f;
+            win[j] = ext[(o0 + j + 2 * K) * LP + l];                    // tap m = -K
+        }
+        // output o0 + j at tap m reads staged position o0 + j + K - m
+        for (int m = -K; m <= K; ++m) {
+            const float gm = taps[m < 0 ? -m : m];
+#pragma unroll
+            for (int j = 0; j < GS_RUN; ++j) acc[j] = fmaf(gm, win[j], acc[j]);
+            if (m < K) {
+#pragma unroll
+                for (int j = GS_RUN - 1; j > 0; --j) win[j] = win[j - 1];
+                win[0] = ext[(o0 + K - m - 1) * LP + l];
+            }
+        }
+        const long long base = line_base(line0 + l);
+#pragma unroll
+        for (int j = 0; j < GS_RUN; ++j) {
+            const int i = i0 + o0 + j;
+            if (i < n && o0 + j < TO) out[base + (long long)i * step] = acc[j];
+        }
+    }
+}
+
+template <int L>
+static size_t gauss_lines_smem(int K, int TO) {
+    return ((size_t)(TO + 2 * K) * (L + 1) + (size_t)(K + 1)) * sizeof(float);
+}
+
 }  // namespace mr
 
 extern "C" int mr_rotate_f32(const float* in, float* out, int32_t rows, int32_t k, int32_t cols,
@@ -87,10 +174,30 @@ extern "C" int mr_gaussian_axis_f32(const float* in, float* out, int32_t rows, i
     if ((axis != 0 && axis != 2) || pad < 0 || n_taps < 1) return MR_ERR_INVALID;
     if (k == 0) return MR_OK;
     if (k > 65535 || rows > 65535) return MR_ERR_INVALID;
-    const dim3 block(128);
-    const dim3 grid((cols + 127) / 128, rows, k);
-    mr::gauss_axis_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
-        in, out, rows, k, cols, axis, pad, taps, n_taps - 1);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int K = n_taps - 1;
+    const int n = axis == 0 ? rows : cols;
+    const long long n_lines = axis == 0 ? (long long)k * cols : (long long)rows * k;
+    constexpr size_t kSmemMax = 200 * 1024;
+    // 32 lines x 128 outputs per block where the staged stretch fits, else 8 lines x 256
+    if (K <= n + 2 * pad && mr::gauss_lines_smem<32>(K, 128) <= kSmemMax) {
+        const size_t smem = mr::gauss_lines_smem<32>(K, 128);
+        MR_CUDA_TRY(cudaFuncSetAttribute(mr::gauss_lines_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+        const dim3 grid((unsigned)((n_lines + 31) / 32), (unsigned)((n + 127) / 128));
+        mr::gauss_lines_kernel<32><<<grid, mr::GS_THREADS, smem, st>>>(in, out, rows, k, cols, axis, pad, taps, K,
+                                                                        128);
+    } else if (K <= n + 2 * pad && mr::gauss_lines_smem<8>(K, 256) <= kSmemMax) {
+        const size_t smem = mr::gauss_lines_smem<8>(K, 256);
+        MR_CUDA_TRY(cudaFuncSetAttribute(mr::gauss_lines_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+        const dim3 grid((unsigned)((n_lines + 7) / 8), (unsigned)((n + 255) / 256));
+        mr::gauss_lines_kernel<8><<<grid, mr::GS_THREADS, smem, st>>>(in, out, rows, k, cols, axis, pad, taps, K, 256);
+    } else {
+        const dim3 block(128);
+        const dim3 grid((cols + 127) / 128, rows, k);
+        mr::gauss_axis_kernel<<<grid, block, 0, st>>>(in, out, rows, k, cols, axis, pad, taps, K);
+    }
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;
 }
