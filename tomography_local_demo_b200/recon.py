@@ -1461,67 +1461,83 @@ class SliceReconstructor:
                              n_views)
 
     def calibrate(self, shift0=None, tilt0=0.0, z=0.0, n=192, fit_tilt=True, iters=60, tol=1e-3,
-                  verbose=False):
+                  heights=(-0.6, -0.3, 0.0, 0.3, 0.6), verbose=False):
         """Gradient-based rotation-centre / detector-tilt calibration.
 
-        Maximises a differentiable histogram score (Gaussian-kernel soft histogram of the
-        axial slice at z and of the central x-z slice, the smooth counterpart of the
-        estimate_cor criterion) over (cor_shift [px], tilt [deg]) by gradient ascent with
-        backtracking; the gradients come from the hand-written backward of the
-        back-projector. Sets the shift (tilt is returned, not stored). Returns
-        (shift, tilt_deg, history)."""
+        The score of a set of slices is a differentiable histogram score (Gaussian-kernel
+        soft histogram of each slice, the smooth counterpart of the estimate_cor criterion
+        sum p log p, recon.py:508-512), maximised by gradient ascent with backtracking; the
+        gradients come from the hand-written backward of the back-projector.
+          1. the COR shift [px] on the axial slice at z - the plane the grid search of
+             estimate_cor scores (recon.py:498-519). It projects onto the central detector
+             rows, where an in-plane detector tilt moves nothing;
+          2. with fit_tilt, the tilt [deg] with the shift held, on axial slices at
+             `heights` x the box half-height: a tilt shows as a COR shift that grows with
+             the distance from the central row, so only slices across the height see it;
+          3. with fit_tilt, the shift again at that tilt.
+        Sets the shift (the tilt is returned, not stored). Returns (shift, tilt_deg,
+        history), history a list of (shift, tilt_deg, score) after every step."""
         from .autograd import backproject, soft_neg_entropy
         ring = self._ring
-        reqs = [dict(origin=(0.0, 0.0, z), normal=(0.0, 0.0, 1.0), n=n),
-                dict(origin=(0.0, 0.0, 0.0), normal=(0.0, 1.0, 0.0), n=n)]
-        op = self.bp_operator(reqs)
-        sizes = [n * n, n * n]
         dev = self.device
         deg = np.pi / 180.0
+        zb = float(self.box[2])
+
+        def objective(zs):
+            reqs = [dict(origin=(0.0, 0.0, float(zz)), normal=(0.0, 0.0, 1.0), n=n) for zz in zs]
+            op = self.bp_operator(reqs)
+            with torch.no_grad():      # histogram ranges fixed from the nominal geometry
+                f0 = backproject(ring, torch.tensor(0.0, dtype=torch.float64),
+                                 torch.tensor(0.0, dtype=torch.float64), op)
+            ranges = []
+            for k in range(len(zs)):
+                part = f0[k * n * n:(k + 1) * n * n]
+                nz = part[part != 0]
+                ranges.append((float(nz.min()), float(nz.max())) if nz.numel() else (0.0, 1.0))
+
+            def score(xv, active):
+                xs = xv.clone().requires_grad_(True)
+                f = backproject(ring, xs[0], xs[1] * deg, op)
+                J = 0.0
+                for k, (lo, hi) in enumerate(ranges):
+                    J = J + soft_neg_entropy(f[k * n * n:(k + 1) * n * n].double(), lo, hi)
+                J.backward()
+                g = xs.grad.clone()
+                g[1 - active] = 0.0
+                return float(J.detach()), g
+            return score
+
+        def ascend(score, x, active, hist):
+            J, g = score(x, active)
+            step = 0.5
+            for _ in range(iters):
+                gmax = float(g.abs().max())
+                if gmax == 0.0:
+                    break
+                d = g / gmax                                   # unit max-norm ascent direction
+                accepted = False
+                while step > tol / 4:
+                    xn = x + step * d
+                    Jn, gn = score(xn, active)
+                    if Jn > J:
+                        x, J, g = xn, Jn, gn
+                        step *= 1.5
+                        accepted = True
+                        break
+                    step *= 0.5
+                hist.append((float(x[0]), float(x[1]), J))
+                if not accepted or step < tol:
+                    break
+            return x
+
         x = torch.tensor([self.cor_shift if shift0 is None else float(shift0), float(tilt0)],
                          dtype=torch.float64, device=dev)
-        with torch.no_grad():
-            f0 = backproject(ring, x[0], x[1] * deg, op)
-        ranges = []
-        o = 0
-        for sz in sizes:
-            nz = f0[o:o + sz][f0[o:o + sz] != 0]
-            ranges.append((float(nz.min()), float(nz.max())) if nz.numel() else (0.0, 1.0))
-            o += sz
-
-        def score(xv, grad=True):
-            xs = xv.clone().requires_grad_(grad)
-            f = backproject(ring, xs[0], xs[1] * deg, op)
-            J, o = 0.0, 0
-            for sz, (lo, hi) in zip(sizes, ranges):
-                J = J + soft_neg_entropy(f[o:o + sz].double(), lo, hi)
-                o += sz
-            if not grad:
-                return float(J.detach()), None
-            J.backward()
-            g = xs.grad.clone()
-            if not fit_tilt:
-                g[1] = 0.0
-            return float(J.detach()), g
-
-        J, g = score(x)
-        step = 0.5
-        hist = [(float(x[0]), float(x[1]), J)]
-        for _ in range(iters):
-            d = g / max(float(g.abs().max()), 1e-30)          # unit max-norm ascent direction
-            accepted = False
-            while step > tol / 4:
-                xn = x + step * d
-                Jn, gn = score(xn)
-                if Jn > J:
-                    x, J, g = xn, Jn, gn
-                    step *= 1.5
-                    accepted = True
-                    break
-                step *= 0.5
-            hist.append((float(x[0]), float(x[1]), J))
-            if not accepted or step < tol:
-                break
+        hist = [(float(x[0]), float(x[1]), float("nan"))]
+        centre = objective([z])
+        x = ascend(centre, x, 0, hist)
+        if fit_tilt:
+            x = ascend(objective([h * zb for h in heights]), x, 1, hist)
+            x = ascend(centre, x, 0, hist)
         self.set_cor_shift(float(x[0]))
         if verbose:
             print(f"[minirecast] calibrated COR shift {float(x[0]):+.3f} px, tilt {float(x[1]):+.4f} deg "
