@@ -15,7 +15,17 @@
 //                        with dcol/dshift = 1, drow/dshift = uv, dcol/dtilt = row - shift uv - cr,
 //                        drow/dtilt = -(col - shift - cc); the distance weight depends on neither.
 // Geometry is recomputed from the per-view maps (nothing from the forward pass is stored).
+//
+// A tile's views may be split over a thread-block cluster of up to 8 CTAs (few tiles: the
+// calibration's slices are a few dozen tiles): each CTA takes a contiguous share of the
+// views; forward partial sums are reduced through distributed shared memory in rank order
+// (deterministic, no scratch), geometry partials go through the FP64 atomics that already
+// combine the tiles, and adjoint taps are scattered atomically either way.
+#include <cooperative_groups.h>
+
 #include "mr_common.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace mr {
 
@@ -35,7 +45,11 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
     __shared__ float s_q[GR_VCH], s_uv[GR_VCH];
     __shared__ mr_grid s_g;
     __shared__ double s_red[2][GR_THREADS / 32];
-    const mr_tile t = tiles[blockIdx.x];
+    __shared__ float4 s_part[GR_THREADS];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank();
+    const int csize = (int)cluster.num_blocks();
+    const mr_tile t = tiles[blockIdx.x / csize];
     const int tid = threadIdx.x;
     if (tid < (int)(sizeof(mr_grid) / 4))
         reinterpret_cast<int*>(&s_g)[tid] = reinterpret_cast<const int*>(grids + t.grid)[tid];
@@ -97,6 +111,12 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
     float ds = 0.f, dt = 0.f;
     int first, nv;                      // slots [first, first + nv)
     grid_view_range(g.view_begin, g.n_views, n_slots, &first, &nv);
+    {                                   // this CTA's share of them
+        const int b = first + (int)(((long long)nv * crank) / csize);
+        const int e = first + (int)(((long long)nv * (crank + 1)) / csize);
+        first = b;
+        nv = e - b;
+    }
     for (int v0 = 0; v0 < nv; v0 += GR_VCH) {
         const int nch = min(GR_VCH, nv - v0);
         __syncthreads();
@@ -165,7 +185,17 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
             }
         }
     }
-    if (MODE == GRAD_FORWARD) {
+    if (MODE == GRAD_FORWARD && csize > 1) {
+        s_part[tid] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        cluster.sync();
+        if (crank == 0) {
+            for (int r = 1; r < csize; ++r) {
+                const float4 o = cluster.map_shared_rank(s_part, r)[tid];
+                acc[0] += o.x; acc[1] += o.y; acc[2] += o.z; acc[3] += o.w;
+            }
+        }
+    }
+    if (MODE == GRAD_FORWARD && crank == 0) {
 #pragma unroll
         for (int p = 0; p < GR_PPT; ++p) {
             const bool ok = pts ? (t.j0 + tid + GR_THREADS * p < g.n_j)
@@ -191,17 +221,35 @@ bp_grad_kernel(const T* __restrict__ ring, float* __restrict__ gring, int R, int
             atomicAdd(dgeom + 2 * t.grid + 1, sb);
         }
     }
+    if (MODE == GRAD_FORWARD && csize > 1) cluster.sync();   // partials stay alive until read
 }
 
 template <int KIND, int MODE, typename T>
 static int launch_grad(const mr_ring* ring, float* gring, const mr_view* views, const mr_grid* grids,
                        const mr_tile* tiles, int64_t n_tiles, const float* gout, double* dgeom, cudaStream_t st) {
-    const int64_t max_chunk = 2147483647LL;
+    // CTAs per tile: enough for about four waves of CTAs on the GPU, at most 8 (portable cluster)
+    int dev = 0, sms = 148;
+    MR_CUDA_TRY(cudaGetDevice(&dev));
+    MR_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    int cl = 1;
+    while (cl < 8 && n_tiles * cl < 4LL * sms) cl *= 2;
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(GR_THREADS);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const int64_t max_chunk = 2147483647LL / cl;
     for (int64_t t0 = 0; t0 < n_tiles; t0 += max_chunk) {
         const int64_t n = (n_tiles - t0) < max_chunk ? (n_tiles - t0) : max_chunk;
-        bp_grad_kernel<KIND, MODE, T><<<(unsigned)n, GR_THREADS, 0, st>>>(
-            static_cast<const T*>(ring->data), gring, ring->rows, ring->cols, ring->col_pitch,
-            (long long)ring->slot_stride, (int)ring->n_slots, views, grids, tiles + t0, gout, dgeom);
+        cfg.gridDim = dim3((unsigned)(n * cl));
+        MR_CUDA_TRY(cudaLaunchKernelEx(&cfg, bp_grad_kernel<KIND, MODE, T>, static_cast<const T*>(ring->data), gring,
+                                       ring->rows, ring->cols, ring->col_pitch, (long long)ring->slot_stride,
+                                       (int)ring->n_slots, views, grids, tiles + t0, gout, dgeom));
     }
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;
