@@ -68,12 +68,13 @@ __global__ void gauss_axis_kernel(const float* __restrict__ in, float* __restric
 // the padded length (the spectrum is cut at Nyquist), so a direct loop costs ~n/2 taps per
 // output. A block takes L lines (rows along axis 2, columns along axis 0) and TO outputs of
 // each: it stages the stretch of the edge-padded, periodically extended line those outputs
-// read - padded positions i0 + pad - K .. i0 + TO - 1 + pad + K - into shared memory once,
-// then every thread slides a window of 8 consecutive outputs of one line over the taps: one
-// shared load and 8 FMAs per tap. Each output sums its taps m = -K .. K in the same order
-// and with the same FMAs as gauss_axis_kernel, so the results are identical.
+// read into shared memory once, then every thread computes 8 consecutive outputs of one
+// line, 8 taps at a time: 15 staged values in registers serve the 64 products of a block of
+// taps. The taps are padded in front with zeros to a multiple of 8 (m from K - 8 nb + 1);
+// those add 0 * x to a zero sum, exactly, so each output is the same FMA chain over
+// m = -K .. K as in gauss_axis_kernel and the results are identical.
 constexpr int GS_THREADS = 256;
-constexpr int GS_RUN = 8;                       // consecutive outputs per thread
+constexpr int GS_RUN = 8;                       // consecutive outputs per thread = taps per block
 
 template <int L>
 __global__ void __launch_bounds__(GS_THREADS)
@@ -81,9 +82,11 @@ gauss_lines_kernel(const float* __restrict__ in, float* __restrict__ out, int R,
                    int pad, const float* __restrict__ g, int K, int TO) {
     extern __shared__ float gsm[];
     constexpr int LP = L + 1;                   // padded line stride: conflict-free stores
-    const int T = TO + 2 * K;                   // staged padded positions per line
-    float* ext = gsm;                           // [T][LP]
-    float* taps = gsm + (size_t)T * LP;         // [K + 1]
+    const int nb = (2 * K + 1 + GS_RUN - 1) / GS_RUN;           // blocks of 8 taps
+    const int m0 = K - GS_RUN * nb + 1;                        // first (zero-padded) tap
+    const int T = TO + GS_RUN * nb;             // staged positions per line
+    float* taps = gsm;                          // [8 nb]: tap m0 + i
+    float* ext = gsm + GS_RUN * nb;             // [T][LP]
     const long long srow = (long long)A * C;
     const int n = axis == 0 ? R : C;
     const int Np = n + 2 * pad;
@@ -96,7 +99,11 @@ gauss_lines_kernel(const float* __restrict__ in, float* __restrict__ out, int R,
         const long long r = line / A, a = line - r * A;
         return r * srow + a * C;
     };
-    for (int m = threadIdx.x; m <= K; m += GS_THREADS) taps[m] = __ldg(g + m);
+    for (int i = threadIdx.x; i < GS_RUN * nb; i += GS_THREADS) {
+        const int m = m0 + i;
+        taps[i] = m < -K ? 0.f : __ldg(g + (m < 0 ? -m : m));
+    }
+    // staged position t holds padded position i0 + pad - K + t; output o at tap m reads t = o + K - m
     const int nl = (int)min((long long)L, n_lines - line0);
     for (int e = threadIdx.x; e < L * T; e += GS_THREADS) {
         int l, t;
@@ -120,35 +127,34 @@ gauss_lines_kernel(const float* __restrict__ in, float* __restrict__ out, int R,
         const int o0 = q * GS_RUN;                                      // first output (block-local)
         if (l >= nl || i0 + o0 >= n) continue;
         float acc[GS_RUN];
-        float win[GS_RUN];
 #pragma unroll
-        for (int j = 0; j < GS_RUN; ++j) {
-            acc[j] = 0.f;
-            win[j] = ext[(o0 + j + 2 * K) * LP + l];                    // tap m = -K
-        }
-        // output o0 + j at tap m reads staged position o0 + j + K - m
-        for (int m = -K; m <= K; ++m) {
-            const float gm = taps[m < 0 ? -m : m];
+        for (int j = 0; j < GS_RUN; ++j) acc[j] = 0.f;
+        for (int b = 0; b < nb; ++b) {
+            // taps m = mb + u (u < 8) of outputs o0 + j read t = o0 + j + K - mb - u
+            const int base = o0 + K - (m0 + GS_RUN * b) - (GS_RUN - 1);
+            float w[2 * GS_RUN - 1];
 #pragma unroll
-            for (int j = 0; j < GS_RUN; ++j) acc[j] = fmaf(gm, win[j], acc[j]);
-            if (m < K) {
+            for (int k = 0; k < 2 * GS_RUN - 1; ++k) w[k] = ext[(base + k) * LP + l];
 #pragma unroll
-                for (int j = GS_RUN - 1; j > 0; --j) win[j] = win[j - 1];
-                win[0] = ext[(o0 + K - m - 1) * LP + l];
+            for (int u = 0; u < GS_RUN; ++u) {
+                const float gm = taps[GS_RUN * b + u];
+#pragma unroll
+                for (int j = 0; j < GS_RUN; ++j) acc[j] = fmaf(gm, w[j - u + GS_RUN - 1], acc[j]);
             }
         }
-        const long long base = line_base(line0 + l);
+        const long long lb = line_base(line0 + l);
 #pragma unroll
         for (int j = 0; j < GS_RUN; ++j) {
             const int i = i0 + o0 + j;
-            if (i < n && o0 + j < TO) out[base + (long long)i * step] = acc[j];
+            if (i < n && o0 + j < TO) out[lb + (long long)i * step] = acc[j];
         }
     }
 }
 
 template <int L>
 static size_t gauss_lines_smem(int K, int TO) {
-    return ((size_t)(TO + 2 * K) * (L + 1) + (size_t)(K + 1)) * sizeof(float);
+    const int nb = (2 * K + 1 + GS_RUN - 1) / GS_RUN;
+    return ((size_t)(TO + GS_RUN * nb) * (L + 1) + (size_t)GS_RUN * nb) * sizeof(float);
 }
 
 }  // namespace mr

@@ -1469,8 +1469,10 @@ class SliceReconstructor:
         sum p log p, recon.py:508-512), maximised by gradient ascent with backtracking; the
         gradients come from the hand-written backward of the back-projector.
           1. the COR shift [px] on the axial slice at z - the plane the grid search of
-             estimate_cor scores (recon.py:498-519). It projects onto the central detector
-             rows, where an in-plane detector tilt moves nothing;
+             estimate_cor scores (recon.py:498-519), which projects onto the central
+             detector rows, where an in-plane detector tilt moves nothing - and the central
+             x-z slice, whose score moves the ascent off a wrong start (a COR error smears
+             every slice);
           2. with fit_tilt, the tilt [deg] with the shift held, on axial slices at
              `heights` x the box half-height: a tilt shows as a COR shift that grows with
              the distance from the central row, so only slices across the height see it;
@@ -1483,14 +1485,14 @@ class SliceReconstructor:
         deg = np.pi / 180.0
         zb = float(self.box[2])
 
-        def objective(zs):
-            reqs = [dict(origin=(0.0, 0.0, float(zz)), normal=(0.0, 0.0, 1.0), n=n) for zz in zs]
+        def objective(planes):
+            reqs = [dict(origin=o, normal=nrm, n=n) for o, nrm in planes]
             op = self.bp_operator(reqs)
             with torch.no_grad():      # histogram ranges fixed from the nominal geometry
                 f0 = backproject(ring, torch.tensor(0.0, dtype=torch.float64),
                                  torch.tensor(0.0, dtype=torch.float64), op)
             ranges = []
-            for k in range(len(zs)):
+            for k in range(len(planes)):
                 part = f0[k * n * n:(k + 1) * n * n]
                 nz = part[part != 0]
                 ranges.append((float(nz.min()), float(nz.max())) if nz.numel() else (0.0, 1.0))
@@ -1533,10 +1535,11 @@ class SliceReconstructor:
         x = torch.tensor([self.cor_shift if shift0 is None else float(shift0), float(tilt0)],
                          dtype=torch.float64, device=dev)
         hist = [(float(x[0]), float(x[1]), float("nan"))]
-        centre = objective([z])
+        axial = (0.0, 0.0, 1.0)
+        centre = objective([((0.0, 0.0, z), axial), ((0.0, 0.0, 0.0), (0.0, 1.0, 0.0))])
         x = ascend(centre, x, 0, hist)
         if fit_tilt:
-            x = ascend(objective([h * zb for h in heights]), x, 1, hist)
+            x = ascend(objective([((0.0, 0.0, h * zb), axial) for h in heights]), x, 1, hist)
             x = ascend(centre, x, 0, hist)
         self.set_cor_shift(float(x[0]))
         if verbose:
