@@ -1461,7 +1461,7 @@ class SliceReconstructor:
                              n_views)
 
     def calibrate(self, shift0=None, tilt0=0.0, z=0.0, n=192, fit_tilt=True, iters=60, tol=1e-3,
-                  heights=(-0.6, -0.3, 0.0, 0.3, 0.6), verbose=False):
+                  heights=(-0.6, 0.6), verbose=False):
         """Gradient-based rotation-centre / detector-tilt calibration.
 
         The score of a set of slices is a differentiable histogram score (Gaussian-kernel
@@ -1475,7 +1475,8 @@ class SliceReconstructor:
              every slice);
           2. with fit_tilt, the tilt [deg] with the shift held, on axial slices at
              `heights` x the box half-height: a tilt shows as a COR shift that grows with
-             the distance from the central row, so only slices across the height see it;
+             the distance from the central row, so the slices far from it see it most
+             (slices near the centre add noise-driven jitter and no tilt signal);
           3. with fit_tilt, the shift again at that tilt.
         Sets the shift (the tilt is returned, not stored). Returns (shift, tilt_deg,
         history), history a list of (shift, tilt_deg, score) after every step."""
