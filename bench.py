@@ -306,8 +306,10 @@ def run_ours(args, rank, world, local):
     gc.disable()
     clocks.mark()
     e0.record(rec.ingest_stream)
+    h0 = time.perf_counter()
     for _ in range(args.steps):
         step_device()
+    t_issue = time.perf_counter() - h0         # host time to issue the steps (the GPU may still run)
     e1.record(rec.stream)
     torch.cuda.synchronize()
     clocks.__exit__(None, None, None)
@@ -369,6 +371,7 @@ def run_ours(args, rank, world, local):
         "e2e": {"value": updates * world * args.steps / t_e2e, "unit": "updates/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": t_e2e / args.steps * 1e3},
+        "host_issue_ms_per_step": t_issue / args.steps * 1e3,
         "gpu_launches": launches,
         "kernels": {k: {"launches": n, "avg_ms": t / n, "share": t / sum(x[1] for x in kern.values())}
                     for k, (n, t) in kern.items()},

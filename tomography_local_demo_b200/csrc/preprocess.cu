@@ -76,12 +76,11 @@ __global__ void gauss_axis_kernel(const float* __restrict__ in, float* __restric
 constexpr int GS_THREADS = 256;
 constexpr int GS_RUN = 8;                       // consecutive outputs per thread = taps per block
 
-template <int L>
+template <int L, int LP>
 __global__ void __launch_bounds__(GS_THREADS)
 gauss_lines_kernel(const float* __restrict__ in, float* __restrict__ out, int R, int A, int C, int axis,
                    int pad, const float* __restrict__ g, int K, int TO) {
     extern __shared__ float gsm[];
-    constexpr int LP = L + 1;                   // padded line stride: conflict-free stores
     const int nb = (2 * K + 1 + GS_RUN - 1) / GS_RUN;           // blocks of 8 taps
     const int m0 = K - GS_RUN * nb + 1;                        // first (zero-padded) tap
     const int T = TO + GS_RUN * nb;             // staged positions per line
@@ -151,10 +150,12 @@ gauss_lines_kernel(const float* __restrict__ in, float* __restrict__ out, int R,
     }
 }
 
-template <int L>
+// LP: the staged line stride (L + 1, or 18 for 16 lines: the two half-warps of a warp,
+// 8 staged positions apart, then fall on opposite halves of the banks)
+template <int LP>
 static size_t gauss_lines_smem(int K, int TO) {
     const int nb = (2 * K + 1 + GS_RUN - 1) / GS_RUN;
-    return ((size_t)(TO + GS_RUN * nb) * (L + 1) + (size_t)GS_RUN * nb) * sizeof(float);
+    return ((size_t)(TO + GS_RUN * nb) * LP + (size_t)GS_RUN * nb) * sizeof(float);
 }
 
 }  // namespace mr
@@ -185,20 +186,23 @@ extern "C" int mr_gaussian_axis_f32(const float* in, float* out, int32_t rows, i
     const int n = axis == 0 ? rows : cols;
     const long long n_lines = axis == 0 ? (long long)k * cols : (long long)rows * k;
     constexpr size_t kSmemMax = 200 * 1024;
-    // 32 lines x 128 outputs per block where the staged stretch fits, else 8 lines x 256
-    if (K <= n + 2 * pad && mr::gauss_lines_smem<32>(K, 128) <= kSmemMax) {
-        const size_t smem = mr::gauss_lines_smem<32>(K, 128);
-        MR_CUDA_TRY(cudaFuncSetAttribute(mr::gauss_lines_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem));
-        const dim3 grid((unsigned)((n_lines + 31) / 32), (unsigned)((n + 127) / 128));
-        mr::gauss_lines_kernel<32><<<grid, mr::GS_THREADS, smem, st>>>(in, out, rows, k, cols, axis, pad, taps, K,
-                                                                        128);
-    } else if (K <= n + 2 * pad && mr::gauss_lines_smem<8>(K, 256) <= kSmemMax) {
-        const size_t smem = mr::gauss_lines_smem<8>(K, 256);
-        MR_CUDA_TRY(cudaFuncSetAttribute(mr::gauss_lines_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    // whole lines per block (16 lines: every input staged about twice, the periodic
+    // extension) where they fit, else 8 lines x 256 outputs
+    const int whole = (n + mr::GS_RUN - 1) / mr::GS_RUN * mr::GS_RUN;
+    if (K <= n + 2 * pad && mr::gauss_lines_smem<18>(K, whole) <= kSmemMax) {
+        const size_t smem = mr::gauss_lines_smem<18>(K, whole);
+        MR_CUDA_TRY(cudaFuncSetAttribute(mr::gauss_lines_kernel<16, 18>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const dim3 grid((unsigned)((n_lines + 15) / 16), 1);
+        mr::gauss_lines_kernel<16, 18><<<grid, mr::GS_THREADS, smem, st>>>(in, out, rows, k, cols, axis, pad, taps,
+                                                                            K, whole);
+    } else if (K <= n + 2 * pad && mr::gauss_lines_smem<9>(K, 256) <= kSmemMax) {
+        const size_t smem = mr::gauss_lines_smem<9>(K, 256);
+        MR_CUDA_TRY(cudaFuncSetAttribute(mr::gauss_lines_kernel<8, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem));
         const dim3 grid((unsigned)((n_lines + 7) / 8), (unsigned)((n + 255) / 256));
-        mr::gauss_lines_kernel<8><<<grid, mr::GS_THREADS, smem, st>>>(in, out, rows, k, cols, axis, pad, taps, K, 256);
+        mr::gauss_lines_kernel<8, 9><<<grid, mr::GS_THREADS, smem, st>>>(in, out, rows, k, cols, axis, pad, taps, K,
+                                                                          256);
     } else {
         const dim3 block(128);
         const dim3 grid((cols + 127) / 128, rows, k);
