@@ -3,6 +3,7 @@
 The library is the only compute path: there is no CPU fallback. If it is missing,
 every call raises RuntimeError naming the build step.
 """
+import collections
 import ctypes
 import os
 import threading
@@ -150,7 +151,32 @@ def tile_shape():
 _TILE_SHAPE = None
 
 
+_PLAN_CACHE = collections.OrderedDict()     # (grid bytes, band axis) -> read-only tile array
+_PLAN_CACHE_MAX = 64
+_PLAN_LOCK = threading.Lock()
+
+
 def plan_tiles(grids, band_axis=None):
+    """plan_tiles_uncached, memoised on the grid records' bytes and the band axis: a
+    repeated request list (a viewer re-slicing, a server replaying, a bench step) reuses
+    its tile list instead of re-planning it on the host. The returned array is read-only."""
+    grids = np.ascontiguousarray(grids, dtype=GRID_DTYPE)
+    key = (grids.tobytes(), None if band_axis is None else tuple(float(x) for x in band_axis))
+    with _PLAN_LOCK:
+        hit = _PLAN_CACHE.get(key)
+        if hit is not None:
+            _PLAN_CACHE.move_to_end(key)
+            return hit
+    tiles = plan_tiles_uncached(grids, band_axis)
+    tiles.flags.writeable = False
+    with _PLAN_LOCK:
+        _PLAN_CACHE[key] = tiles
+        if len(_PLAN_CACHE) > _PLAN_CACHE_MAX:
+            _PLAN_CACHE.popitem(last=False)
+    return tiles
+
+
+def plan_tiles_uncached(grids, band_axis=None):
     """Tiles (numpy TILE_DTYPE array) covering the grids (numpy GRID_DTYPE array).
 
     band_axis: the orbit's rotation axis (the detector's row direction). When given, the

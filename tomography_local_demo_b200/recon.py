@@ -11,6 +11,7 @@ FP64 is used on the host only, to build the per-view projective maps and the fil
 spectrum (as the reference does); the device computes in FP32 and stores the filtered
 views in FP32 (default), BF16 or FP16.
 """
+import collections
 import ctypes
 import threading
 import time
@@ -1281,6 +1282,23 @@ class SliceReconstructor:
         shift = self.cor_shift if cor_shift is None else float(cor_shift)
         return plane_grid(self.box, origin, normal, int(n), size, zoom, center, shift)
 
+    def _plane_record(self, origin, normal, n, size, zoom, center, shift):
+        """plane_grid for this reconstructor's box, memoised on the request's parameters
+        (the FP64 plane set-up is pure; a repeated request skips it on the host)."""
+        flat = lambda v: None if v is None else tuple(float(x) for x in np.ravel(v))   # noqa: E731
+        key = (flat(origin), flat(normal), int(n), None if size is None else float(size), float(zoom),
+               flat(center), float(shift))
+        cache = self.__dict__.setdefault("_plane_cache", collections.OrderedDict())
+        rec = cache.get(key)
+        if rec is None:
+            rec = plane_grid(self.box, origin, normal, n, size, zoom, center, shift)
+            cache[key] = rec
+            if len(cache) > 256:
+                cache.popitem(last=False)
+        else:
+            cache.move_to_end(key)
+        return rec.copy()
+
     def _planes(self, requests):
         """One batched launch for many slices -> (flat f32 device tensor, sizes)."""
         n_views, shift, ev = self._snapshot()
@@ -1289,9 +1307,9 @@ class SliceReconstructor:
         for r, req in enumerate(requests):
             n = int(req.get("n", 256))
             s_ = req.get("cor_shift")
-            grids[r] = plane_grid(self.box, req["origin"], req["normal"], n, req.get("size"),
-                                  req.get("zoom", 1.0), req.get("center"),
-                                  shift if s_ is None else float(s_))
+            grids[r] = self._plane_record(req["origin"], req["normal"], n, req.get("size"),
+                                          req.get("zoom", 1.0), req.get("center"),
+                                          shift if s_ is None else float(s_))
             grids[r]["out_offset"] = offset
             sizes.append(n)
             offset += n * n
