@@ -1495,7 +1495,9 @@ class SliceReconstructor:
              `heights` x the box half-height: a tilt shows as a COR shift that grows with
              the distance from the central row, so the slices far from it see it most
              (slices near the centre add noise-driven jitter and no tilt signal);
-          3. with fit_tilt, the shift again at that tilt.
+          3. with fit_tilt, the shift again at that tilt; steps 2 and 3 alternate until
+             neither moves by more than `tol` (the best tilt of the outer slices depends on
+             the shift they are seen with).
         Sets the shift (the tilt is returned, not stored). Returns (shift, tilt_deg,
         history), history a list of (shift, tilt_deg, score) after every step."""
         from .autograd import backproject, soft_neg_entropy
@@ -1558,8 +1560,13 @@ class SliceReconstructor:
         centre = objective([((0.0, 0.0, z), axial), ((0.0, 0.0, 0.0), (0.0, 1.0, 0.0))])
         x = ascend(centre, x, 0, hist)
         if fit_tilt:
-            x = ascend(objective([((0.0, 0.0, h * zb), axial) for h in heights]), x, 1, hist)
-            x = ascend(centre, x, 0, hist)
+            outer = objective([((0.0, 0.0, h * zb), axial) for h in heights])
+            for _ in range(6):
+                prev = x.clone()
+                x = ascend(outer, x, 1, hist)
+                x = ascend(centre, x, 0, hist)
+                if float((x - prev).abs().max()) < 10 * tol:
+                    break
         self.set_cor_shift(float(x[0]))
         if verbose:
             print(f"[minirecast] calibrated COR shift {float(x[0]):+.3f} px, tilt {float(x[1]):+.4f} deg "
