@@ -527,6 +527,10 @@ def serving_simulation(args, dev, geom, raw_dev, flats, darks):
     srv.latencies.clear()
     srv.latency_kinds.clear()
     srv.updates = 0
+    # as in the other timed regions, no cyclic garbage collection while the scan runs: a
+    # full collection pauses every thread of the process, the server's included
+    gc.collect()
+    gc.disable()
     t0 = time.perf_counter()
     next_req = t0 + rng.exponential(1.0 / req_rate)
     pushed, sent = 0, 0                 # groups and views pushed so far
@@ -548,6 +552,7 @@ def serving_simulation(args, dev, geom, raw_dev, flats, darks):
     for f in futs + previews:
         f.result()
     wall = time.perf_counter() - t0
+    gc.enable()
     srv.device_status()
     srv.close()
     st = srv.stats()
