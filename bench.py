@@ -9,7 +9,9 @@ arbitrarily oriented 512 x 512 slices (seeded random unit normals, offsets withi
 +/-10 mm) are back-projected from all 600 views in one batched launch.
 
 Metric: voxel-projection updates/s = (in-box slice pixels x views) / step time.
-  value : device time with the raw counts already resident in HBM (CUDA events)
+  value : device time with the raw counts already resident in HBM (CUDA events), the
+          step replayed from a captured CUDA graph (SliceReconstructor.scan_replay); the
+          same step issued eagerly through the public calls is reported under "eager"
   e2e   : the public API with pinned host buffers (H2D of the raw counts, D2H of the
           three images inside the timed region), host wall clock
 Multi-GPU (torchrun): every rank runs its own scan (independent objects, no
@@ -312,13 +314,32 @@ def run_ours(args, rank, world, local):
     t_issue = time.perf_counter() - h0         # host time to issue the steps (the GPU may still run)
     e1.record(rec.stream)
     torch.cuda.synchronize()
-    clocks.__exit__(None, None, None)
     gc.enable()
     barrier(world)
     rec.kernel_timer = None
-    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3, world, dev)
+    t_eager = max_over_ranks(e0.elapsed_time(e1) / 1e3, world, dev)
     kern = timer.summary()
-    launches = sum(n for n, _ in kern.values())
+
+    # ---- the same step replayed from a captured CUDA graph (ScanReplay: the ingest and
+    # the batched back-projection, no host work between steps); this is the device
+    # throughput, free of the host's issue time, which the eager loop above exposes when
+    # the host is slower than the device
+    replay = rec.scan_replay(raw_dev, reqs)
+    for _ in range(args.warmup):
+        replay.replay()
+    torch.cuda.synchronize()
+    barrier(world)
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(replay.stream)
+    for _ in range(args.steps):
+        replay.replay()
+    g1.record(replay.stream)
+    torch.cuda.synchronize()
+    clocks.__exit__(None, None, None)
+    barrier(world)
+    t_dev = max_over_ranks(g0.elapsed_time(g1) / 1e3, world, dev)
+    launches = 2 * args.steps                 # one ingest and one back-projection per replay
+    del replay
 
     # ---- end to end through the public API, pinned host buffers
     raw_host = torch.empty(raw_dev.shape, dtype=torch.int16, pin_memory=True)
@@ -371,7 +392,9 @@ def run_ours(args, rank, world, local):
         "e2e": {"value": updates * world * args.steps / t_e2e, "unit": "updates/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": t_e2e / args.steps * 1e3},
-        "host_issue_ms_per_step": t_issue / args.steps * 1e3,
+        "eager": {"ms_per_step": t_eager / args.steps * 1e3, "host_issue_ms_per_step": t_issue / args.steps * 1e3,
+                  "note": "the same step through reset / add_raw_projections / reconstruct_planes_tensor, "
+                          "issued from the host each step; its launches give the per-kernel times"},
         "gpu_launches": launches,
         "kernels": {k: {"launches": n, "avg_ms": t / n, "share": t / sum(x[1] for x in kern.values())}
                     for k, (n, t) in kern.items()},
@@ -401,6 +424,7 @@ def _traffic(kernel):
 
 
 def roofline(name, stats, updates, store):
+    from tomography_local_demo_b200.recon import ring_pitch
     n, t_ms = stats
     avg = t_ms / n / 1e3
     peaks = {}
@@ -420,7 +444,7 @@ def roofline(name, stats, updates, store):
         peak = peaks.get("bf16_tflops", 1590.0)
         ach = flops / avg / 1e12
         out_b = 2 if store != "fp32" else 4
-        pitch = (w["cols"] + 7) // 8 * 8
+        pitch = ring_pitch(w["cols"], store)
         alg_bytes = w["views"] * w["rows"] * (w["cols"] * 2 + pitch * out_b)
         return {"kernel": name, "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
                 "frac": ach / peak, "traffic": _traffic(name), "executed_flops": flops,
@@ -431,7 +455,7 @@ def roofline(name, stats, updates, store):
     if name == "mr_ingest_u16":
         w = WORKLOAD
         out_b = 2 if store != "fp32" else 4
-        pitch = (w["cols"] + 7) // 8 * 8
+        pitch = ring_pitch(w["cols"], store)
         alg = w["views"] * w["rows"] * (w["cols"] * 2 + pitch * out_b)
         peak = peaks.get("hbm_gbs", 6650.0)
         ach = alg / avg / 1e9
@@ -457,26 +481,30 @@ def bp_only_and_latency(args, dev, geom, raw_dev, flats, darks, reqs, updates, r
     rec32.add_raw_projections(idx, raw_dev)
     reps = max(args.steps, 5)
 
-    def timed(fn, stream):
+    from tomography_local_demo_b200.recon import KernelTimer
+
+    def timed(fn, rec):
+        """Back-projection time per call: the device time of the call's launches (CUDA
+        events right around each launch), so that the host's issue time between calls does
+        not enter the comparison of the kernels."""
         for _ in range(3):
             fn()
         torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
+        rec.kernel_timer = KernelTimer()
         for _ in range(reps):
             fn()
-        b.record(stream)
-        torch.cuda.synchronize()
-        return a.elapsed_time(b) / 1e3 / reps
+        kern = rec.kernel_timer.summary()
+        rec.kernel_timer = None
+        return sum(t for _, t in kern.values()) / 1e3 / reps
 
-    t32 = timed(lambda: [rec32.reconstruct_planes_tensor([r]) for r in reqs], rec32.stream)
+    t32 = timed(lambda: [rec32.reconstruct_planes_tensor([r]) for r in reqs], rec32)
     rec_bf16.reset()
     rec_bf16.add_raw_projections(idx, raw_dev)
-    tbf = timed(lambda: rec_bf16.reconstruct_planes_tensor(reqs), rec_bf16.stream)
-    t32b = timed(lambda: rec32.reconstruct_planes_tensor(reqs), rec32.stream)
+    tbf = timed(lambda: rec_bf16.reconstruct_planes_tensor(reqs), rec_bf16)
+    t32b = timed(lambda: rec32.reconstruct_planes_tensor(reqs), rec32)
     # the plain FP32 GPU path: direct global gathers (mr_backproject), one request per launch
     rec32.bp_kernel = "plain"
-    t32p = timed(lambda: [rec32.reconstruct_planes_tensor([r]) for r in reqs], rec32.stream)
+    t32p = timed(lambda: [rec32.reconstruct_planes_tensor([r]) for r in reqs], rec32)
     rec32.bp_kernel = "staged"
     # per-request latency of the 3-slice batch through the public API (host wall clock,
     # includes descriptor upload and the D2H of the images)

@@ -189,6 +189,29 @@ __device__ __forceinline__ float2 ldg_f2_now(const void* p) {
     return v;
 }
 
+__device__ __forceinline__ void st_global_v4(unsigned char* p, const uint32_t* w) {
+    *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+}
+__device__ __forceinline__ void st_global_v8(unsigned char* p, const uint32_t* w) {
+    asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(w[0]), "r"(w[1]),
+                 "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7])
+                 : "memory");
+}
+// NW 4-byte words to p (16-byte aligned), as far as `room` bytes reach: 32-byte stores
+// where p is 32-byte aligned (a32) and the piece fits, 16-byte stores otherwise.
+template <int NW>
+__device__ __forceinline__ void store_row_words(unsigned char* p, const uint32_t* w, int room, bool a32) {
+#pragma unroll
+    for (int j = 0; j < NW / 8; ++j) {
+        if (a32 && 32 * j + 32 <= room) {
+            st_global_v8(p + 32 * j, w + 8 * j);
+        } else {
+            if (32 * j + 16 <= room) st_global_v4(p + 32 * j, w + 8 * j);
+            if (32 * j + 32 <= room) st_global_v4(p + 32 * j + 16, w + 8 * j + 4);
+        }
+    }
+}
+
 // Byte offset of element (row, k) (k even: a pair of 16-bit values) in a SWIZZLE_128B
 // K-major tile: 16-byte chunk index XOR (row mod 8) inside each 128-byte row.
 __device__ __forceinline__ uint32_t swz(int row, int k) {
@@ -204,14 +227,14 @@ __device__ __forceinline__ void split2(float2 x, uint32_t& hi, uint32_t& lo) {
             x.y = fminf(fmaxf(x.y, -65504.f), 65504.f);
         }
         const __half2 h = __floats2half2_rn(x.x, x.y);
-        const float2 hf = __half22float2(h);
-        const __half2 l = __floats2half2_rn(x.x - hf.x, x.y - hf.y);
+        const float2 d = __ffma2_rn(__half22float2(h), make_float2(-1.f, -1.f), x);     // x - hi, exact
+        const __half2 l = __floats2half2_rn(d.x, d.y);
         hi = *reinterpret_cast<const uint32_t*>(&h);
         lo = *reinterpret_cast<const uint32_t*>(&l);
     } else {
         const __nv_bfloat162 h = __floats2bfloat162_rn(x.x, x.y);
-        const float2 hf = __bfloat1622float2(h);
-        const __nv_bfloat162 l = __floats2bfloat162_rn(x.x - hf.x, x.y - hf.y);
+        const float2 d = __ffma2_rn(__bfloat1622float2(h), make_float2(-1.f, -1.f), x);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(d.x, d.y);
         hi = *reinterpret_cast<const uint32_t*>(&h);
         lo = *reinterpret_cast<const uint32_t*>(&l);
     }
@@ -448,24 +471,28 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                         if (cin && ((vmask >> i) & 1u)) {
                             if (RAW) {
                                 const uint32_t w = reinterpret_cast<const uint32_t*>(cur)[i];
-                                x.x = __log2f(fmaxf(fmaf((float)(w & 0xFFFFu), gn_c.x, nd.x), 1e-3f));
-                                x.y = __log2f(fmaxf(fmaf((float)(w >> 16), gn_c.y, nd.y), 1e-3f));
+                                // the counts as floats without the conversion unit (which the
+                                // logarithms need): 2^23 + n carries n in its low mantissa bits,
+                                // so subtracting 2^23 gives n exactly
+                                const float2 m = make_float2(__uint_as_float(0x4B000000u | (w & 0xFFFFu)),
+                                                             __uint_as_float(0x4B000000u | (w >> 16)));
+                                const float2 t = __ffma2_rn(__fadd2_rn(m, make_float2(-8388608.f, -8388608.f)), gn_c, nd);
+                                x.x = __log2f(fmaxf(t.x, 1e-3f));
+                                x.y = __log2f(fmaxf(t.y, 1e-3f));
                             } else {
                                 x = reinterpret_cast<const float2*>(cur)[i];
                             }
-                            float k1 = k1u, k2 = k2u;
+                            float2 kk = make_float2(k1u, k2u);
                             if (!uni) {
                                 const RowInfo ri = my_rows[i];
-                                k1 = ri.kx;
-                                k2 = ri.kx;
+                                kk = make_float2(ri.kx, ri.kx);
                                 if (ri.sdd != 0.f) {
                                     const float a1 = fmaf(fc1, ri.da, ri.a0), a2 = fmaf(fc2, ri.da, ri.a0);
-                                    k1 *= rsqrtf(fmaf(a1, a1, ri.s2b));
-                                    k2 *= rsqrtf(fmaf(a2, a2, ri.s2b));
+                                    kk.x *= rsqrtf(fmaf(a1, a1, ri.s2b));
+                                    kk.y *= rsqrtf(fmaf(a2, a2, ri.s2b));
                                 }
                             }
-                            x.x *= k1;
-                            x.y *= k2;
+                            x = __fmul2_rn(x, kk);
                         }
                         uint32_t hi, lo;
                         // raw counts: |x| < 11.1 * 1024 by construction, no FP16 range clamp needed
@@ -595,6 +622,7 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                 out = static_cast<unsigned char*>(A.ring) +
                       ((long long)fv.slot * A.slot_stride + (long long)r * A.pitch) * esz;
             }
+            const bool a32 = (reinterpret_cast<uintptr_t>(out) & 31u) == 0;
             const int nch = (A.pitch + 31) / 32;
             const int nld = (NCOL / 32 < nch) ? NCOL / 32 : nch;         // chunks inside the accumulator
             const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
@@ -608,21 +636,20 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                 }
 #pragma unroll
                 for (int e = 0; e < 32; ++e) vv[e] = (32 * ch + e < A.cols) ? vv[e] * scale : 0.f;
-                // each lane stores its own row (view) as 16-byte segments: the L2 merges the
-                // partial sectors, and the warp spends no shared-memory round trip on a
-                // transpose (a staged transpose into coalesced rows measured 6 % slower)
+                // each lane stores its own row (view): the warp spends no shared-memory round
+                // trip on a transpose (a staged transpose into coalesced rows measured 6 %
+                // slower), and the L2 merges the sectors. A warp's store touches 32 rows, so
+                // the number of stores, not the bytes, sets the cost: 32-byte stores where the
+                // row start is 32-byte aligned, 16-byte ones elsewhere and at the row's end
                 if (live) {
                     const int esz = A.dtype == MR_F32 ? 4 : 2;
-                    const int per = 16 / esz;
+                    const int room = (A.pitch - 32 * ch) * esz;             // bytes left in the row
+                    unsigned char* p = out + 32 * ch * esz;
                     if (A.dtype == MR_F32) {
+                        uint32_t w[32];
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int col = 32 * ch + 4 * j;
-                            if (col + per <= A.pitch)
-                                *reinterpret_cast<uint4*>(out + col * esz) =
-                                    make_uint4(__float_as_uint(vv[4 * j]), __float_as_uint(vv[4 * j + 1]),
-                                               __float_as_uint(vv[4 * j + 2]), __float_as_uint(vv[4 * j + 3]));
-                        }
+                        for (int e = 0; e < 32; ++e) w[e] = __float_as_uint(vv[e]);
+                        store_row_words<32>(p, w, room, a32);
                     } else {
                         uint32_t w[16];
 #pragma unroll
@@ -635,13 +662,7 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_tc_kernel(Args A) {
                                 w[e] = *reinterpret_cast<const uint32_t*>(&pk);
                             }
                         }
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int col = 32 * ch + 8 * j;
-                            if (col + per <= A.pitch)
-                                *reinterpret_cast<uint4*>(out + col * esz) =
-                                    make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
-                        }
+                        store_row_words<16>(p, w, room, a32);
                     }
                 }
             }
