@@ -364,24 +364,23 @@ bp_staged_kernel(const __grid_constant__ CUtensorMap tmap, const T* __restrict__
                     meta_new[lane] = view_meta<KIND, T>(views[v_begin + vb + lane], g, ox, oy, oz, di_max,
                                                         dj_max, R, C);
                 __syncwarp();
-                if (lane == 0) {
-                    for (int l = 0; l < cnt; ++l) {
-                        const uint32_t ua = used + (uint32_t)(vb + l);      // absolute stage use
-                        const int s = (int)(ua % S);
-                        const uint32_t u = ua / S;
+                // lane 0 frees and arms the stage, then lane b issues the copy of box b: the
+                // boxes of a view go out in one warp instruction instead of one after another
+                for (int l = 0; l < cnt; ++l) {
+                    const uint32_t ua = used + (uint32_t)(vb + l);          // absolute stage use
+                    const int s = (int)(ua % S);
+                    const uint32_t u = ua / S;
+                    const int mode = meta_new[l].mode, nbox = meta_new[l].nbox;
+                    if (lane == 0) {
                         if (u > 0) mbar_wait(&empty[s], (u - 1) & 1u, status);
-                        const ViewMeta m = meta_new[l];
-                        meta_ring[s] = m.rec;
-                        if (m.mode == MODE_STAGED) {
-                            mbar_arrive_tx(&full[s], (uint32_t)(m.nbox * BOX_BYTES));
-                            unsigned char* dst = stages + s * STAGE_BYTES;
-                            for (int b = 0; b < m.nbox; ++b)
-                                tma_load_3d(dst + b * BOX_BYTES, &tmap, m.x0, m.r0 + b * ST_BOX_H,
-                                            v_begin + vb + l, &full[s]);
-                        } else {
-                            mbar_arrive(&full[s]);
-                        }
+                        meta_ring[s] = meta_new[l].rec;
+                        if (mode == MODE_STAGED) mbar_arrive_tx(&full[s], (uint32_t)(nbox * BOX_BYTES));
+                        else mbar_arrive(&full[s]);
                     }
+                    __syncwarp();                   // the stage is free and armed for every lane
+                    if (mode == MODE_STAGED && lane < nbox)
+                        tma_load_3d(stages + s * STAGE_BYTES + lane * BOX_BYTES, &tmap, meta_new[l].x0,
+                                    meta_new[l].r0 + lane * ST_BOX_H, v_begin + vb + l, &full[s]);
                 }
             }
         }
