@@ -326,8 +326,9 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // PREF: the next item's two input rows are copied to shared memory with cp.async while the
 // current item's FFTs run (bin 1 only; rows of 4-byte aligned, 4-byte multiple length).
-template <int LOG2N, bool RAW, bool PREF>
-__global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A) {
+// SMF: the CTA's dark / gain rows sit in shared memory (every CTA works on one row pair).
+template <int LOG2N, bool RAW, bool PREF, bool SMF>
+__global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int split) {
     using P = fft::Plan<LOG2N>;
     constexpr int N = P::N, G = P::G, FPB = P::FPB;
     constexpr int ES = RAW ? 2 : 4;                      // input element size
@@ -350,11 +351,22 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A) {
     __syncthreads();
 
     const int R = A.rows, C = A.cols;
-    const int pairs = (R + 1) / 2;
-    const long long n_items = (long long)A.k * pairs;
-    const long long stride = (long long)gridDim.x * FPB;
-    // item = pair * k + view: the FPB FFT slots of a CTA take FPB views of the same row
-    // pair, so dark/gain rows are shared through L1
+    // CTA b filters row pair b / split, views (b % split) * FPB + f + m * split * FPB of it:
+    // all its FFT slots share the pair's dark / gain rows
+    const int pair = blockIdx.x / split;
+    const int vstride = split * FPB;
+    const long long n_items = (long long)A.k * ((R + 1) / 2);
+    float* fld = reinterpret_cast<float*>(pref - f * 2 * row_bytes + FPB * 2 * row_bytes);   // [4][C]
+    if (RAW && SMF) {
+        // dark of rows 2 pair, 2 pair + 1, then gain of the same rows
+        for (int e = threadIdx.x; e < 4 * C; e += blockDim.x) {
+            const int q = e / C, c = e - q * C;
+            const int r = 2 * pair + (q & 1);
+            fld[e] = r < R ? __ldg(((q >> 1) ? A.gain : A.dark) + (long long)r * C + c) : 0.f;
+        }
+        __syncthreads();
+    }
+    // item = pair * k + view
     auto src_row = [&](long long item, int row) -> const unsigned char* {
         const int pr = (int)(item / A.k);
         const int v = (int)(item - (long long)pr * A.k);
@@ -377,13 +389,15 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A) {
         }
         if (PREF) cp_async_commit();
     };
-    prefetch((long long)blockIdx.x * FPB + f);
-    for (long long base = (long long)blockIdx.x * FPB; base < n_items; base += stride) {
-        const long long item = base + f;
-        const bool live = item < n_items;              // uniform per FFT group
-        const int pr = live ? (int)(item / A.k) : 0;
-        const int v = live ? (int)(item - (long long)pr * A.k) : 0;
-        const int r1 = 2 * pr;
+    const int v_first = (blockIdx.x % split) * FPB;
+    const long long item0 = (long long)pair * A.k;
+    if (v_first + f < A.k) prefetch(item0 + v_first + f);
+    else if (PREF) cp_async_commit();
+    for (int vb = v_first; vb < A.k; vb += vstride) {
+        const bool live = vb + f < A.k;                // uniform per FFT group
+        const long long item = item0 + vb + f;
+        const int v = live ? vb + f : 0;
+        const int r1 = 2 * pair;
         const mr_filter_view fv = A.views[v];
         if (PREF) {
             cp_async_wait_all();
@@ -408,10 +422,14 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A) {
                     if (RAW) {
                         const int pix = r1 * A.cols + c;
                         const float s1 = (float)reinterpret_cast<const uint16_t*>(pref)[c];
-                        x1 = -__logf(fmaxf((s1 - __ldg(A.dark + pix)) * __ldg(A.gain + pix), 1e-3f));
+                        const float d1 = SMF ? fld[c] : __ldg(A.dark + pix);
+                        const float g1 = SMF ? fld[2 * C + c] : __ldg(A.gain + pix);
+                        x1 = -__logf(fmaxf((s1 - d1) * g1, 1e-3f));
                         if (r1 + 1 < R) {
                             const float s2r = (float)reinterpret_cast<const uint16_t*>(pref + row_bytes)[c];
-                            x2 = -__logf(fmaxf((s2r - __ldg(A.dark + pix + A.cols)) * __ldg(A.gain + pix + A.cols), 1e-3f));
+                            const float d2 = SMF ? fld[C + c] : __ldg(A.dark + pix + A.cols);
+                            const float g2 = SMF ? fld[3 * C + c] : __ldg(A.gain + pix + A.cols);
+                            x2 = -__logf(fmaxf((s2r - d2) * g2, 1e-3f));
                         }
                     } else {
                         x1 = reinterpret_cast<const float*>(pref)[c];
@@ -428,7 +446,8 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A) {
         }
         if (PREF) {
             fft::fft_sync<G>();                         // everyone has read the staged rows
-            prefetch(item + stride);
+            if (vb + vstride + f < A.k) prefetch(item + vstride);
+            else cp_async_commit();
         }
 #pragma unroll
         for (int q = 16; q < 32; ++q) x[q] = make_float2(0.f, 0.f);
@@ -486,17 +505,21 @@ static int launch_fft_filter(const Filter2Args& A, cudaStream_t st) {
                       A.s_row % elem_align == 0 &&
                       (reinterpret_cast<uintptr_t>(RAW ? (const void*)A.raw : (const void*)A.block) & 3) == 0 &&
                       base_smem + pref_smem <= 200 * 1024;
-    const size_t smem = base_smem + (pref ? pref_smem : 0);
-    auto kern = pref ? fft_filter_kernel<LOG2N, RAW, true> : fft_filter_kernel<LOG2N, RAW, false>;
+    // the dark / gain rows of the CTA's row pair in shared memory when two CTAs still fit an SM
+    const size_t fld_smem = (size_t)4 * A.cols * sizeof(float);
+    const bool smf = RAW && pref && base_smem + pref_smem + fld_smem <= 112 * 1024;
+    const size_t smem = base_smem + (pref ? pref_smem : 0) + (smf ? fld_smem : 0);
+    auto kern = smf ? fft_filter_kernel<LOG2N, RAW, true, true>
+                    : (pref ? fft_filter_kernel<LOG2N, RAW, true, false> : fft_filter_kernel<LOG2N, RAW, false, false>);
     MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int dev = 0, sms = 148;
-    MR_CUDA_TRY(cudaGetDevice(&dev));
-    MR_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const long long items = (long long)A.k * ((A.rows + 1) / 2);
-    const long long need = (items + P::FPB - 1) / P::FPB;
-    const long long grid = need < 2LL * sms * 8 ? need : 2LL * sms * 8;
-    if (grid <= 0) return MR_OK;
-    kern<<<(unsigned)grid, 256, smem, st>>>(A);
+    // one row pair per CTA, its views split over `split` CTAs of FPB FFT slots: about eight
+    // views a slot
+    const long long pairs = (A.rows + 1) / 2;
+    const long long split = (A.k + 8LL * P::FPB - 1) / (8LL * P::FPB);
+    const long long grid = pairs * split;
+    if (A.k <= 0 || grid <= 0) return MR_OK;
+    if (grid > 2147483647LL) return MR_ERR_UNSUPPORTED;
+    kern<<<(unsigned)grid, 256, smem, st>>>(A, (int)split);
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;
 }
