@@ -357,12 +357,38 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
     const int vstride = split * FPB;
     const long long n_items = (long long)A.k * ((R + 1) / 2);
     float* fld = reinterpret_cast<float*>(pref - f * 2 * row_bytes + FPB * 2 * row_bytes);   // [4][C]
+    float* wtab = fld + 4 * C;                     // [2][C] FDK weights of the CTA's first view
+    float* wkey = wtab + 2 * C;                    // that view's a0, da, b0, db, sdd
     if (RAW && SMF) {
         // dark of rows 2 pair, 2 pair + 1, then gain of the same rows
         for (int e = threadIdx.x; e < 4 * C; e += blockDim.x) {
             const int q = e / C, c = e - q * C;
             const int r = 2 * pair + (q & 1);
             fld[e] = r < R ? __ldg(((q >> 1) ? A.gain : A.dark) + (long long)r * C + c) : 0.f;
+        }
+        // the cosine weights of the pair's rows for the constants of the CTA's first view:
+        // the views of one orbit usually share them, and a view that does reads its
+        // weights here instead of computing them (the same operations, the same values)
+        const int v0 = min((int)(blockIdx.x % split) * FPB, A.k - 1);
+        const mr_filter_view f0 = A.views[v0];
+        for (int e = threadIdx.x; e < 2 * C; e += blockDim.x) {
+            const int q = e / C, c = e - q * C;
+            float w = 1.f;
+            if (f0.sdd != 0.f) {
+                const float aa = fmaf((float)c, f0.da, f0.a0);
+                const float b1 = fmaf((float)(2 * pair), f0.db, f0.b0);
+                const float b = q ? b1 + f0.db : b1;
+                const float s2 = fmaf(f0.sdd, f0.sdd, aa * aa);
+                w = f0.sdd * rsqrtf(fmaf(b, b, s2));
+            }
+            wtab[e] = w;
+        }
+        if (threadIdx.x == 0) {
+            wkey[0] = f0.a0;
+            wkey[1] = f0.da;
+            wkey[2] = f0.b0;
+            wkey[3] = f0.db;
+            wkey[4] = f0.sdd;
         }
         __syncthreads();
     }
@@ -404,13 +430,18 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
             fft::fft_sync<G>();                         // the staged rows are visible to the group
         }
         float2 x[32];
+        const bool tab = RAW && SMF && fv.a0 == wkey[0] && fv.da == wkey[1] && fv.b0 == wkey[2] &&
+                         fv.db == wkey[3] && fv.sdd == wkey[4];
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
             const int c = j + G * q;
             float a = 0.f, b = 0.f;
             if (live && c < C) {
                 float w1 = 1.f, w2 = 1.f;
-                if (fv.sdd != 0.f) {
+                if (tab) {
+                    w1 = wtab[c];
+                    w2 = wtab[C + c];
+                } else if (fv.sdd != 0.f) {
                     const float aa = fmaf((float)c, fv.da, fv.a0);
                     const float b1 = fmaf((float)r1, fv.db, fv.b0), b2 = b1 + fv.db;
                     const float s2 = fmaf(fv.sdd, fv.sdd, aa * aa);
@@ -506,7 +537,7 @@ static int launch_fft_filter(const Filter2Args& A, cudaStream_t st) {
                       (reinterpret_cast<uintptr_t>(RAW ? (const void*)A.raw : (const void*)A.block) & 3) == 0 &&
                       base_smem + pref_smem <= 200 * 1024;
     // the dark / gain rows of the CTA's row pair in shared memory when two CTAs still fit an SM
-    const size_t fld_smem = (size_t)4 * A.cols * sizeof(float);
+    const size_t fld_smem = (size_t)6 * A.cols * sizeof(float) + 8 * sizeof(float);
     const bool smf = RAW && pref && base_smem + pref_smem + fld_smem <= 112 * 1024;
     const size_t smem = base_smem + (pref ? pref_smem : 0) + (smf ? fld_smem : 0);
     auto kern = smf ? fft_filter_kernel<LOG2N, RAW, true, true>
