@@ -351,10 +351,12 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
     __syncthreads();
 
     const int R = A.rows, C = A.cols;
-    // CTA b filters row pair b / split, views (b % split) * FPB + f + m * split * FPB of it:
-    // all its FFT slots share the pair's dark / gain rows
-    const int pair = blockIdx.x / split;
-    const int vstride = split * FPB;
+    // item = pair * k + view. SMF: CTA b filters row pair b / split, views (b % split) * FPB
+    // + f + m * split * FPB of it, so all its FFT slots share the pair's dark / gain rows,
+    // held in shared memory. Otherwise the CTAs stride over all items (FPB consecutive
+    // views of one pair at a time, the dark / gain rows shared through L1), which keeps
+    // every SM busy to the end when few CTAs fit.
+    const int pair = SMF ? (int)(blockIdx.x / split) : 0;
     const long long n_items = (long long)A.k * ((R + 1) / 2);
     float* fld = reinterpret_cast<float*>(pref - f * 2 * row_bytes + FPB * 2 * row_bytes);   // [4][C]
     float* wtab = fld + 4 * C;                     // [2][C] FDK weights of the CTA's first view
@@ -415,15 +417,18 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
         }
         if (PREF) cp_async_commit();
     };
-    const int v_first = (blockIdx.x % split) * FPB;
-    const long long item0 = (long long)pair * A.k;
-    if (v_first + f < A.k) prefetch(item0 + v_first + f);
+    const long long start = SMF ? (long long)pair * A.k + (long long)(blockIdx.x % split) * FPB
+                                : (long long)blockIdx.x * FPB;
+    const long long end = SMF ? (long long)(pair + 1) * A.k : n_items;
+    const long long step = SMF ? (long long)split * FPB : (long long)gridDim.x * FPB;
+    if (start + f < end) prefetch(start + f);
     else if (PREF) cp_async_commit();
-    for (int vb = v_first; vb < A.k; vb += vstride) {
-        const bool live = vb + f < A.k;                // uniform per FFT group
-        const long long item = item0 + vb + f;
-        const int v = live ? vb + f : 0;
-        const int r1 = 2 * pair;
+    for (long long base = start; base < end; base += step) {
+        const long long item = base + f;
+        const bool live = item < end;                  // uniform per FFT group
+        const int pr = SMF ? pair : (live ? (int)(item / A.k) : 0);
+        const int v = live ? (int)(item - (long long)pr * A.k) : 0;
+        const int r1 = 2 * pr;
         const mr_filter_view fv = A.views[v];
         if (PREF) {
             cp_async_wait_all();
@@ -477,7 +482,7 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
         }
         if (PREF) {
             fft::fft_sync<G>();                         // everyone has read the staged rows
-            if (vb + vstride + f < A.k) prefetch(item + vstride);
+            if (item + step < end) prefetch(item + step);
             else cp_async_commit();
         }
 #pragma unroll
@@ -543,11 +548,18 @@ static int launch_fft_filter(const Filter2Args& A, cudaStream_t st) {
     auto kern = smf ? fft_filter_kernel<LOG2N, RAW, true, true>
                     : (pref ? fft_filter_kernel<LOG2N, RAW, true, false> : fft_filter_kernel<LOG2N, RAW, false, false>);
     MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    // one row pair per CTA, its views split over `split` CTAs of FPB FFT slots: about eight
-    // views a slot
+    // SMF: one row pair per CTA, its views split over `split` CTAs of FPB FFT slots (about
+    // eight views a slot); else a grid of two waves of eight CTAs per SM striding over all
     const long long pairs = (A.rows + 1) / 2;
     const long long split = (A.k + 8LL * P::FPB - 1) / (8LL * P::FPB);
-    const long long grid = pairs * split;
+    long long grid = pairs * split;
+    if (!smf) {
+        int dev = 0, sms = 148;
+        MR_CUDA_TRY(cudaGetDevice(&dev));
+        MR_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const long long need = ((long long)A.k * pairs + P::FPB - 1) / P::FPB;
+        grid = need < 2LL * sms * 8 ? need : 2LL * sms * 8;
+    }
     if (A.k <= 0 || grid <= 0) return MR_OK;
     if (grid > 2147483647LL) return MR_ERR_UNSUPPORTED;
     kern<<<(unsigned)grid, 256, smem, st>>>(A, (int)split);
