@@ -408,6 +408,8 @@ def run_ours(args, rank, world, local):
     line.update(extra)
     if rank == 0 and not args.no_serve:
         line["serving"] = serving_simulation(args, dev, geom, raw_dev, flats, darks)
+        line["serving_fp32_one_request_per_launch"] = serving_simulation(args, dev, geom, raw_dev, flats, darks,
+                                                                         store="fp32", max_batch=1)
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"], line["accuracy"] = cpu_baseline_and_accuracy(
             args, geom, raw_dev, flats, darks, reqs, box, updates, imgs)
@@ -529,19 +531,21 @@ def bp_only_and_latency(args, dev, geom, raw_dev, flats, darks, reqs, updates, r
     }
 
 
-def serving_simulation(args, dev, geom, raw_dev, flats, darks):
+def serving_simulation(args, dev, geom, raw_dev, flats, darks, store="bf16", max_batch=128):
     """Live-scan serving: the scan's raw views stream into the ring at 200 views/s (groups
     of 10) while slice requests arrive as a Poisson process at 500 req/s (sizes uniform in
     {128, 256, 512, 1024}^2, zoom 1-8, random orientation, COR offsets within +/-10 px),
-    plus a 128^3 preview every 50 views; a continuously batched SliceServer (BF16 ring,
-    20 GB admission budget) answers them. Reports p50/p99 submit-to-host latency."""
+    plus a 128^3 preview every 50 views; a SliceServer (20 GB admission budget) answers
+    them: continuously batched on a BF16 ring by default, or one request per launch
+    (max_batch=1) on an FP32 ring for the comparison. The request stream is the same
+    seeded sequence for both. Reports p50/p99 submit-to-host latency and updates/s."""
     import torch
     from tomography_local_demo_b200 import SliceReconstructor
     from tomography_local_demo_b200.server import SliceServer
     from tomography_local_demo_b200.stream import AcquisitionSchedule
-    rec = SliceReconstructor(None, geom, store="bf16", verbose=False, device=dev, filter=args.filter)
+    rec = SliceReconstructor(None, geom, store=store, verbose=False, device=dev, filter=args.filter)
     rec.set_flat_dark(as_u16(flats), as_u16(darks))
-    srv = SliceServer(rec, budget_bytes=20e9, max_batch=128, pool_bytes=1 << 30)
+    srv = SliceServer(rec, budget_bytes=20e9, max_batch=max_batch, pool_bytes=1 << 30)
     rng = np.random.default_rng(5)
     V, rate, req_rate = WORKLOAD["views"], 200.0, 500.0
     sched = AcquisitionSchedule(V, "interleaved", group=10, rate=rate)
@@ -589,7 +593,9 @@ def serving_simulation(args, dev, geom, raw_dev, flats, darks):
             "slice_p99_ms": st["slice_p99_ms"], "wall_s": wall,
             "updates_per_s": st["updates"] / wall,
             "setup": "600 raw views at 200 views/s, Poisson 500 req/s, n in {128..1024}, zoom 1-8, "
-                     "COR +/-10 px, 128^3 preview per 50 views, bf16 ring, 20 GB budget"}
+                     f"COR +/-10 px, 128^3 preview per 50 views, {store} ring, "
+                     + ("continuous batching" if max_batch > 1 else "one request per launch")
+                     + ", 20 GB budget"}
 
 
 def cpu_whole_job(raw, fl, dk, geom, reqs, box, reps, warmup=1, precision="ref"):
