@@ -317,3 +317,14 @@ def test_acquisition_schedule_and_feeder():
     f.stop()
     f.join(5)
     assert not f.is_alive() and f.stopped and len(slow.calls) <= 1
+
+
+def test_ring_pitch_rows_start_32_byte_aligned():
+    """The ring's row pitch is the smallest multiple of 32 bytes holding the row, for every
+    store type (the tensor-core filter stores each row in 32-byte pieces)."""
+    for cols in (1, 7, 8, 15, 16, 17, 486, 488, 496, 512, 1944):
+        for store, esz in (("fp32", 4), ("bf16", 2), ("fp16", 2)):
+            p = R.ring_pitch(cols, store)
+            assert p >= cols and (p * esz) % 32 == 0
+            assert p - 32 // esz < cols                   # the smallest such multiple
+    assert R.ring_pitch(486, "bf16") == 496 and R.ring_pitch(486, "fp32") == 488
