@@ -561,7 +561,7 @@ def serving_simulation(args, dev, geom, raw_dev, flats, darks, store="bf16", max
     V, rate, req_rate = WORKLOAD["views"], 200.0, 500.0
     sched = AcquisitionSchedule(V, "interleaved", group=10, rate=rate)
     futs, previews = [], []
-    # warm the server (first replay captures the graphs)
+    # warm the server (first launches of each request kind: tile plans, module loading)
     first = sched.groups[0]
     rec.add_raw_projections(first, raw_dev[torch.from_numpy(first).to(dev)])
     for f in [srv.submit((0, 0, 0), (0, 0, 1), n=n) for n in (128, 1024)] + [srv.submit_preview(128)]:

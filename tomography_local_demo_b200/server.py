@@ -79,6 +79,13 @@ class SliceServer:
         self.pool_floats = int(pool_bytes) // 4
         self.use_graphs = use_graphs
         self.slots = [_Slot(self.dev, self.max_batch, self.max_tiles, self.pool_floats) for _ in range(slots)]
+        if use_graphs:
+            # every slot's graph is captured here, before the first request: a capture
+            # synchronises the device and collects the interpreter's garbage, a pause of
+            # tens of milliseconds that would otherwise land on whichever request first
+            # reaches each slot
+            for slot in self.slots:
+                self._capture(slot)
         self.queue = collections.deque()
         self.cv = threading.Condition()
         self.in_flight = 0
@@ -183,6 +190,16 @@ class SliceServer:
                 for r in batch:
                     r.future.set_exception(e)
 
+    def _capture(self, slot):
+        """Capture the slot's persistent launch in a CUDA graph (on the slot's stream). The
+        launch reads its batch from the slot's device buffers, so one graph serves every
+        batch the slot takes."""
+        with torch.cuda.device(self.dev), torch.cuda.stream(slot.stream):
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=slot.stream, capture_error_mode="thread_local"):
+                self._graph_launch(slot)
+        slot.graph = g
+
     def _graph_launch(self, slot):
         rec = self.rec
         v = ctypes_void
@@ -222,10 +239,7 @@ class SliceServer:
             if n_views > 0 and len(tiles) > 0:
                 if self.use_graphs:
                     if slot.graph is None:
-                        g = torch.cuda.CUDAGraph()
-                        with torch.cuda.graph(g, stream=st, capture_error_mode="thread_local"):
-                            self._graph_launch(slot)
-                        slot.graph = g
+                        self._capture(slot)
                     slot.graph.replay()
                 else:
                     self._graph_launch(slot)
