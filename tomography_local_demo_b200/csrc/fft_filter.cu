@@ -363,8 +363,9 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
     float* wkey = wtab + 2 * C;                    // that view's a0, da, b0, db, sdd
     if (RAW && SMF) {
         // dark of rows 2 pair, 2 pair + 1, then gain of the same rows
+        // one float4 a column: dark of rows 2 pair, 2 pair + 1, gain of the same rows
         for (int e = threadIdx.x; e < 4 * C; e += blockDim.x) {
-            const int q = e / C, c = e - q * C;
+            const int q = e & 3, c = e >> 2;
             const int r = 2 * pair + (q & 1);
             fld[e] = r < R ? __ldg(((q >> 1) ? A.gain : A.dark) + (long long)r * C + c) : 0.f;
         }
@@ -373,8 +374,8 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
         // weights here instead of computing them (the same operations, the same values)
         const int v0 = min((int)(blockIdx.x % split) * FPB, A.k - 1);
         const mr_filter_view f0 = A.views[v0];
-        for (int e = threadIdx.x; e < 2 * C; e += blockDim.x) {
-            const int q = e / C, c = e - q * C;
+        for (int e = threadIdx.x; e < 2 * C; e += blockDim.x) {      // one float2 a column
+            const int q = e & 1, c = e >> 1;
             float w = 1.f;
             if (f0.sdd != 0.f) {
                 const float aa = fmaf((float)c, f0.da, f0.a0);
@@ -444,8 +445,9 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
             if (live && c < C) {
                 float w1 = 1.f, w2 = 1.f;
                 if (tab) {
-                    w1 = wtab[c];
-                    w2 = wtab[C + c];
+                    const float2 w = reinterpret_cast<const float2*>(wtab)[c];
+                    w1 = w.x;
+                    w2 = w.y;
                 } else if (fv.sdd != 0.f) {
                     const float aa = fmaf((float)c, fv.da, fv.a0);
                     const float b1 = fmaf((float)r1, fv.db, fv.b0), b2 = b1 + fv.db;
@@ -458,14 +460,21 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
                     if (RAW) {
                         const int pix = r1 * A.cols + c;
                         const float s1 = (float)reinterpret_cast<const uint16_t*>(pref)[c];
-                        const float d1 = SMF ? fld[c] : __ldg(A.dark + pix);
-                        const float g1 = SMF ? fld[2 * C + c] : __ldg(A.gain + pix);
-                        x1 = -__logf(fmaxf((s1 - d1) * g1, 1e-3f));
+                        float4 dg = make_float4(0.f, 0.f, 0.f, 0.f);      // dark 1, dark 2, gain 1, gain 2
+                        if (SMF) {
+                            dg = reinterpret_cast<const float4*>(fld)[c];
+                        } else {
+                            dg.x = __ldg(A.dark + pix);
+                            dg.z = __ldg(A.gain + pix);
+                        }
+                        x1 = -__logf(fmaxf((s1 - dg.x) * dg.z, 1e-3f));
                         if (r1 + 1 < R) {
                             const float s2r = (float)reinterpret_cast<const uint16_t*>(pref + row_bytes)[c];
-                            const float d2 = SMF ? fld[C + c] : __ldg(A.dark + pix + A.cols);
-                            const float g2 = SMF ? fld[3 * C + c] : __ldg(A.gain + pix + A.cols);
-                            x2 = -__logf(fmaxf((s2r - d2) * g2, 1e-3f));
+                            if (!SMF) {
+                                dg.y = __ldg(A.dark + pix + A.cols);
+                                dg.w = __ldg(A.gain + pix + A.cols);
+                            }
+                            x2 = -__logf(fmaxf((s2r - dg.y) * dg.w, 1e-3f));
                         }
                     } else {
                         x1 = reinterpret_cast<const float*>(pref)[c];
