@@ -119,9 +119,21 @@ struct Plan {
     static constexpr int BUF = N + N / 32;                             // padded float2 per FFT
 };
 
+// Synchronises the G threads of one FFT (blocks of 256 threads, groups of whole warps):
+// a warp barrier up to 32 threads, a named barrier per group (ids 1 .. 256 / G; 0 is
+// __syncthreads) when several groups share the block, so one group's passes do not wait
+// for the other groups' shared-memory transposes.
 template <int G>
 __device__ __forceinline__ void fft_sync() {
-    if constexpr (G <= 32) __syncwarp(); else __syncthreads();
+    static_assert(G % 32 == 0 || G < 32, "groups are whole warps");
+    if constexpr (G <= 32) {
+        __syncwarp();
+    } else if constexpr (G < 256) {
+        static_assert(256 / G <= 15, "named barrier ids 1..15");
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)(threadIdx.x / G)), "n"(G) : "memory");
+    } else {
+        __syncthreads();
+    }
 }
 
 // Forward FFT of the 32 values v[r] = x[j + G r] of the thread's FFT; on return
