@@ -105,6 +105,29 @@ def test_raw_ingest_matches_flexray_correction_plus_fdk(cuda, bin_, flip):
     assert rel_l2(got, want) < 2e-6
 
 
+@pytest.mark.parametrize("cols,flip", [(700, False), (1944, True)])
+def test_raw_ingest_wide_rows(cuda, cols, flip):
+    """2048- and 4096-point rows: the ingest keeps each CTA on one row pair with the pair's
+    dark / gain rows in shared memory next to float exchange buffers. Odd row count (the last
+    pair has one row), more views than one CTA's slots, per-pixel fields."""
+    from oracle import geometry as og
+    rng = np.random.default_rng(cols)
+    rows, k = 5, 37
+    d_b = rng.normal(100, 5, (rows, cols)).astype(np.float32)
+    g_b = (1.0 / rng.normal(49900, 800, (rows, cols))).astype(np.float32)
+    atten = rng.uniform(0.05, 3.0, (k, rows, cols))
+    raw = (rng.poisson(49900 * np.exp(-atten)) + 100).clip(0, 65535).astype(np.uint16)
+    # a flipped read takes the frame's rows bottom-up; dark / gain are given in output order
+    src = raw[:, ::-1, :] if flip else raw
+    d_f, g_f = (d_b[::-1].copy(), g_b[::-1].copy()) if flip else (d_b, g_b)
+    x = -np.log(np.clip((src.astype(np.float32) - d_f) * g_f, 1e-3, None))
+    V = og.circular_cone_vectors(k, 440.0, 680.0, 0.0748 * 1944 / cols)
+    want = of.fdk_filter_block(np.transpose(x, (1, 0, 2)).astype(np.float32), of.cone_constants(V), "ram-lak",
+                               exact64=True)
+    got = _ingest(raw, d_f, g_f, 1, flip, R.cone_constants(V), rows, cols, "ram-lak")
+    assert rel_l2(got, want) < 2e-6
+
+
 def test_raw_ingest_bf16_store(cuda):
     from oracle import geometry as og
     rng = np.random.default_rng(0)

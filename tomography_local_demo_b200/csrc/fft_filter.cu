@@ -223,29 +223,54 @@ __device__ __forceinline__ void fft32xN(float2 (&v)[32], float2* buf, const floa
 // N >= 1024: passes 1 and 2 are both radix 32; they share one copy of the DIF code in a
 // runtime loop (straight-line radix-32 code is ~7 KB of SASS; four inlined copies
 // thrash the instruction cache). Same input/output contract as fft32xN.
-template <int LOG2N>
+// SPLIT: the FFT's exchange buffer holds N + N/32 floats instead of float2s, and each
+// transpose moves the real parts, then the imaginary parts (two more barriers, the same
+// values in the same registers): half the shared memory, so that the row pair's dark /
+// gain rows fit beside two CTAs an SM at 2048 and 4096 points.
+template <int LOG2N, bool SPLIT = false>
 __device__ __forceinline__ void fft_compact(float2 (&v)[32], float2* buf, const float2* __restrict__ T,
                                             const float2* __restrict__ twN, int j) {
     using P = Plan<LOG2N>;
     constexpr int N = P::N, G = P::G, R3 = P::R3;
     static_assert(P::R2 == 32, "compact path needs N >= 1024");
     const int k = j & 31;
+    float* bf = reinterpret_cast<float*>(buf);
 #pragma unroll 1
     for (int pass = 0; pass < 2; ++pass) {
         if (pass == 1) {
             fft_sync<G>();
+            if constexpr (SPLIT) {
+                // real parts were stored at the end of pass 0; the imaginary parts of the
+                // pass-0 results are still in v[].y
 #pragma unroll
-            for (int r = 0; r < 32; ++r) {
-                float2 x = buf[pad(j + (N / 32) * r)];
-                if (r > 0) x = cmul(x, T[r * 32 + k]);
-                v[r] = x;
+                for (int r = 0; r < 32; ++r) v[r].x = bf[pad(j + (N / 32) * r)];
+                fft_sync<G>();
+#pragma unroll
+                for (int q = 0; q < 32; ++q) bf[pad(32 * j + q)] = v[bitrev(q, 5)].y;
+                fft_sync<G>();
+#pragma unroll
+                for (int r = 0; r < 32; ++r) v[r].y = bf[pad(j + (N / 32) * r)];
+#pragma unroll
+                for (int r = 1; r < 32; ++r) v[r] = cmul(v[r], T[r * 32 + k]);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 32; ++r) {
+                    float2 x = buf[pad(j + (N / 32) * r)];
+                    if (r > 0) x = cmul(x, T[r * 32 + k]);
+                    v[r] = x;
+                }
             }
         }
         dif<32, 0, 1>(v);
         if (pass == 0) {
             fft_sync<G>();
+            if constexpr (SPLIT) {
 #pragma unroll
-            for (int q = 0; q < 32; ++q) buf[pad(32 * j + q)] = v[bitrev(q, 5)];
+                for (int q = 0; q < 32; ++q) bf[pad(32 * j + q)] = v[bitrev(q, 5)].x;
+            } else {
+#pragma unroll
+                for (int q = 0; q < 32; ++q) buf[pad(32 * j + q)] = v[bitrev(q, 5)];
+            }
         }
     }
     if constexpr (R3 == 1) {
@@ -255,20 +280,43 @@ __device__ __forceinline__ void fft_compact(float2 (&v)[32], float2* buf, const 
 #pragma unroll
         for (int m = 0; m < 32; ++m) v[m] = t[m];
     } else {
-        fft_sync<G>();
-#pragma unroll
-        for (int m = 0; m < 32; ++m) buf[pad((j >> 5) * 1024 + k + 32 * m)] = v[bitrev(m, 5)];
-        fft_sync<G>();
         constexpr int NB3 = 32 / R3;
         constexpr int L3 = ilog2(R3);
+        fft_sync<G>();
+        if constexpr (SPLIT) {
 #pragma unroll
-        for (int b = 0; b < NB3; ++b) {
-            const int jj = j + G * b;
+            for (int m = 0; m < 32; ++m) bf[pad((j >> 5) * 1024 + k + 32 * m)] = v[bitrev(m, 5)].x;
+            fft_sync<G>();
 #pragma unroll
-            for (int r = 0; r < R3; ++r) {
-                float2 x = buf[pad(jj + (N / R3) * r)];
-                if (r > 0) x = cmul(x, __ldg(twN + r * jj));
-                v[b * R3 + r] = x;
+            for (int b = 0; b < NB3; ++b)
+#pragma unroll
+                for (int r = 0; r < R3; ++r) v[b * R3 + r].x = bf[pad(j + G * b + (N / R3) * r)];
+            fft_sync<G>();
+#pragma unroll
+            for (int m = 0; m < 32; ++m) bf[pad((j >> 5) * 1024 + k + 32 * m)] = v[bitrev(m, 5)].y;
+            fft_sync<G>();
+#pragma unroll
+            for (int b = 0; b < NB3; ++b) {
+                const int jj = j + G * b;
+#pragma unroll
+                for (int r = 0; r < R3; ++r) {
+                    v[b * R3 + r].y = bf[pad(jj + (N / R3) * r)];
+                    if (r > 0) v[b * R3 + r] = cmul(v[b * R3 + r], __ldg(twN + r * jj));
+                }
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < 32; ++m) buf[pad((j >> 5) * 1024 + k + 32 * m)] = v[bitrev(m, 5)];
+            fft_sync<G>();
+#pragma unroll
+            for (int b = 0; b < NB3; ++b) {
+                const int jj = j + G * b;
+#pragma unroll
+                for (int r = 0; r < R3; ++r) {
+                    float2 x = buf[pad(jj + (N / R3) * r)];
+                    if (r > 0) x = cmul(x, __ldg(twN + r * jj));
+                    v[b * R3 + r] = x;
+                }
             }
         }
 #pragma unroll
@@ -283,10 +331,11 @@ __device__ __forceinline__ void fft_compact(float2 (&v)[32], float2* buf, const 
     }
 }
 
-template <int LOG2N>
+template <int LOG2N, bool SPLIT = false>
 __device__ __forceinline__ void fft_any(float2 (&v)[32], float2* buf, const float2* __restrict__ T,
                                         const float2* __restrict__ twN, int j) {
-    if constexpr (LOG2N >= 10) fft_compact<LOG2N>(v, buf, T, twN, j);
+    static_assert(!SPLIT || LOG2N >= 10, "split exchanges only on the compact path");
+    if constexpr (LOG2N >= 10) fft_compact<LOG2N, SPLIT>(v, buf, T, twN, j);
     else fft32xN<LOG2N, false>(v, buf, T, twN, j);
 }
 
@@ -339,7 +388,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // PREF: the next item's two input rows are copied to shared memory with cp.async while the
 // current item's FFTs run (bin 1 only; rows of 4-byte aligned, 4-byte multiple length).
 // SMF: the CTA's dark / gain rows sit in shared memory (every CTA works on one row pair).
-template <int LOG2N, bool RAW, bool PREF, bool SMF>
+// SPLIT: float exchange buffers (fft_compact), which leave room for those rows at N >= 2048.
+template <int LOG2N, bool RAW, bool PREF, bool SMF, bool SPLIT = false>
 __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int split) {
     using P = fft::Plan<LOG2N>;
     constexpr int N = P::N, G = P::G, FPB = P::FPB;
@@ -348,9 +398,11 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
     float2* T = sm2;                                  // 32 x 32: T[a*32+k] = W_1024^(a k)
     const int f = threadIdx.x / G;
     const int j = threadIdx.x % G;
-    float2* buf = sm2 + 1024 + f * P::BUF;
+    constexpr int BUF_ES = SPLIT ? 4 : 8;               // bytes per exchange-buffer element
+    unsigned char* bufs = reinterpret_cast<unsigned char*>(sm2 + 1024);
+    float2* buf = reinterpret_cast<float2*>(bufs + (size_t)f * P::BUF * BUF_ES);
     const int row_bytes = ((A.cols * ES + 15) / 16) * 16;
-    unsigned char* pref = reinterpret_cast<unsigned char*>(sm2 + 1024 + FPB * P::BUF) + f * 2 * row_bytes;
+    unsigned char* pref = bufs + (size_t)FPB * P::BUF * BUF_ES + f * 2 * row_bytes;
 
     if constexpr (P::R2 > 1) {
         // W_1024^(a k) = W_N^(a k N / 1024); for N < 1024 only a multiple of 1024/N is used
@@ -512,7 +564,7 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
         // forward FFT, conj(H X), forward FFT again (= N * conj of the inverse): one call site
 #pragma unroll 1
         for (int it = 0; it < 2; ++it) {
-            fft::fft_any<LOG2N>(x, buf, T, A.tw, j);
+            fft::fft_any<LOG2N, SPLIT>(x, buf, T, A.tw, j);
             if (it == 0) {
 #pragma unroll
                 for (int q = 0; q < 32; ++q) {
@@ -554,6 +606,7 @@ static int launch_fft_filter(const Filter2Args& A, cudaStream_t st) {
     using P = fft::Plan<LOG2N>;
     constexpr int ES = RAW ? 2 : 4;
     const size_t base_smem = (1024 + (size_t)P::FPB * P::BUF) * sizeof(float2);
+    const size_t split_smem = 1024 * sizeof(float2) + (size_t)P::FPB * P::BUF * sizeof(float);
     const size_t row_bytes = ((size_t)A.cols * ES + 15) / 16 * 16;
     const size_t pref_smem = (size_t)P::FPB * 2 * row_bytes;
     // staged input rows need bin 1 and 4-byte aligned rows of a 4-byte multiple length
@@ -564,10 +617,15 @@ static int launch_fft_filter(const Filter2Args& A, cudaStream_t st) {
                       base_smem + pref_smem <= 200 * 1024;
     // the dark / gain rows of the CTA's row pair in shared memory when two CTAs still fit an SM
     const size_t fld_smem = (size_t)6 * A.cols * sizeof(float) + 8 * sizeof(float);
-    const bool smf = RAW && pref && base_smem + pref_smem + fld_smem <= 112 * 1024;
-    const size_t smem = base_smem + (pref ? pref_smem : 0) + (smf ? fld_smem : 0);
-    auto kern = smf ? fft_filter_kernel<LOG2N, RAW, true, true>
-                    : (pref ? fft_filter_kernel<LOG2N, RAW, true, false> : fft_filter_kernel<LOG2N, RAW, false, false>);
+    bool smf = RAW && pref && base_smem + pref_smem + fld_smem <= 112 * 1024;
+    // 2048 / 4096 points: with float exchange buffers the fields fit beside two CTAs an SM
+    const bool split_smf = RAW && LOG2N >= 11 && LOG2N <= 12 && pref && !smf &&
+                           split_smem + pref_smem + fld_smem <= 112 * 1024;
+    smf = smf || split_smf;
+    const size_t smem = (split_smf ? split_smem : base_smem) + (pref ? pref_smem : 0) + (smf ? fld_smem : 0);
+    auto kern = split_smf ? fft_filter_kernel<LOG2N, RAW, true, true, (RAW && LOG2N >= 11 && LOG2N <= 12)>
+              : smf       ? fft_filter_kernel<LOG2N, RAW, true, true>
+              : (pref ? fft_filter_kernel<LOG2N, RAW, true, false> : fft_filter_kernel<LOG2N, RAW, false, false>);
     MR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // SMF: one row pair per CTA, its views split over `split` CTAs of FPB FFT slots (about
     // eight views a slot); else a grid of two waves of eight CTAs per SM striding over all
