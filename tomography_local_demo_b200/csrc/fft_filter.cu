@@ -220,6 +220,29 @@ __device__ __forceinline__ void fft32xN(float2 (&v)[32], float2* buf, const floa
     }
 }
 
+// x W_32^K for any K < 32 (W_32^(K + 16) = -W_32^K), compile-time constants.
+template <int K>
+__device__ __forceinline__ float2 tw32(float2 x) {
+    if constexpr (K >= 16) {
+        const float2 y = twiddle<32, K - 16>(x);
+        return make_float2(-y.x, -y.y);
+    } else {
+        return twiddle<32, K>(x);
+    }
+}
+// v[b R3 + r] *= W_N^(r j) W_32^(r b) for r > 0, b < 32 / R3 (wj[r] = W_N^(r j)).
+template <int R3, int B = 0, int RR = 1>
+__device__ __forceinline__ void tw3_apply(float2 (&v)[32], const float2 (&wj)[R3]) {
+    if constexpr (B < 32 / R3) {
+        if constexpr (RR < R3) {
+            v[B * R3 + RR] = tw32<(RR * B) % 32>(cmul(v[B * R3 + RR], wj[RR]));
+            tw3_apply<R3, B, RR + 1>(v, wj);
+        } else {
+            tw3_apply<R3, B + 1, 1>(v, wj);
+        }
+    }
+}
+
 // N >= 1024: passes 1 and 2 are both radix 32; they share one copy of the DIF code in a
 // runtime loop (straight-line radix-32 code is ~7 KB of SASS; four inlined copies
 // thrash the instruction cache). Same input/output contract as fft32xN.
@@ -282,6 +305,13 @@ __device__ __forceinline__ void fft_compact(float2 (&v)[32], float2* buf, const 
     } else {
         constexpr int NB3 = 32 / R3;
         constexpr int L3 = ilog2(R3);
+        // SPLIT: W_N^(r (j + G b)) = W_N^(r j) W_32^(r b) (N = 32 G): R3 - 1 table reads a
+        // thread instead of one per value, and a compile-time rotation
+        float2 wj[R3];
+        if constexpr (SPLIT) {
+#pragma unroll
+            for (int r = 1; r < R3; ++r) wj[r] = __ldg(twN + r * j);
+        }
         fft_sync<G>();
         if constexpr (SPLIT) {
 #pragma unroll
@@ -299,11 +329,9 @@ __device__ __forceinline__ void fft_compact(float2 (&v)[32], float2* buf, const 
             for (int b = 0; b < NB3; ++b) {
                 const int jj = j + G * b;
 #pragma unroll
-                for (int r = 0; r < R3; ++r) {
-                    v[b * R3 + r].y = bf[pad(jj + (N / R3) * r)];
-                    if (r > 0) v[b * R3 + r] = cmul(v[b * R3 + r], __ldg(twN + r * jj));
-                }
+                for (int r = 0; r < R3; ++r) v[b * R3 + r].y = bf[pad(jj + (N / R3) * r)];
             }
+            tw3_apply<R3>(v, wj);
         } else {
 #pragma unroll
             for (int m = 0; m < 32; ++m) buf[pad((j >> 5) * 1024 + k + 32 * m)] = v[bitrev(m, 5)];
@@ -391,6 +419,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // SPLIT: float exchange buffers (fft_compact), which leave room for those rows at N >= 2048.
 template <int LOG2N, bool RAW, bool PREF, bool SMF, bool SPLIT = false>
 __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int split) {
+    static_assert(!SPLIT || (RAW && PREF && SMF), "split exchanges come with the pair's fields");
     using P = fft::Plan<LOG2N>;
     constexpr int N = P::N, G = P::G, FPB = P::FPB;
     constexpr int ES = RAW ? 2 : 4;                      // input element size
@@ -425,6 +454,11 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
     float* fld = reinterpret_cast<float*>(pref - f * 2 * row_bytes + FPB * 2 * row_bytes);   // [4][C]
     float* wtab = fld + 4 * C;                     // [2][C] FDK weights of the CTA's first view
     float* wkey = wtab + 2 * C;                    // that view's a0, da, b0, db, sdd
+    // SPLIT: H[0 .. N/2] (the spectrum is even, H[n] = H[N - n] bit for bit) after the key
+    float* hs = wkey + 8;
+    if constexpr (SPLIT) {
+        for (int e = threadIdx.x; e <= N / 2; e += blockDim.x) hs[e] = __ldg(A.H + e);
+    }
     if (RAW && SMF) {
         // dark of rows 2 pair, 2 pair + 1, then gain of the same rows
         // one float4 a column: dark of rows 2 pair, 2 pair + 1, gain of the same rows
@@ -568,7 +602,9 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
             if (it == 0) {
 #pragma unroll
                 for (int q = 0; q < 32; ++q) {
-                    const float h = __ldg(A.H + j + G * q) * g;
+                    // n = j + G q is below N/2 exactly when q < 16
+                    const float hn = SPLIT ? (q < 16 ? hs[j + G * q] : hs[N - j - G * q]) : __ldg(A.H + j + G * q);
+                    const float h = hn * g;
                     x[q] = __fmul2_rn(x[q], make_float2(h, -h));
                 }
             }
@@ -618,11 +654,14 @@ static int launch_fft_filter(const Filter2Args& A, cudaStream_t st) {
     // the dark / gain rows of the CTA's row pair in shared memory when two CTAs still fit an SM
     const size_t fld_smem = (size_t)6 * A.cols * sizeof(float) + 8 * sizeof(float);
     bool smf = RAW && pref && base_smem + pref_smem + fld_smem <= 112 * 1024;
-    // 2048 / 4096 points: with float exchange buffers the fields fit beside two CTAs an SM
+    // 2048 / 4096 points: with float exchange buffers the fields (and half the spectrum)
+    // fit beside two CTAs an SM
+    const size_t hs_smem = (size_t)(P::N / 2 + 1) * sizeof(float);
     const bool split_smf = RAW && LOG2N >= 11 && LOG2N <= 12 && pref && !smf &&
-                           split_smem + pref_smem + fld_smem <= 112 * 1024;
+                           split_smem + pref_smem + fld_smem + hs_smem <= 112 * 1024;
     smf = smf || split_smf;
-    const size_t smem = (split_smf ? split_smem : base_smem) + (pref ? pref_smem : 0) + (smf ? fld_smem : 0);
+    const size_t smem = (split_smf ? split_smem + hs_smem : base_smem) + (pref ? pref_smem : 0) +
+                        (smf ? fld_smem : 0);
     auto kern = split_smf ? fft_filter_kernel<LOG2N, RAW, true, true, (RAW && LOG2N >= 11 && LOG2N <= 12)>
               : smf       ? fft_filter_kernel<LOG2N, RAW, true, true>
               : (pref ? fft_filter_kernel<LOG2N, RAW, true, false> : fft_filter_kernel<LOG2N, RAW, false, false>);
