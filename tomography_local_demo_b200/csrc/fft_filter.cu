@@ -413,6 +413,11 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
+// FP32 value -> ring element (round to nearest for the 16-bit rings)
+__device__ __forceinline__ float ring_cvt(const float*, float y) { return y; }
+__device__ __forceinline__ __nv_bfloat16 ring_cvt(const __nv_bfloat16*, float y) { return __float2bfloat16_rn(y); }
+__device__ __forceinline__ __half ring_cvt(const __half*, float y) { return __float2half_rn(y); }
+
 // PREF: the next item's two input rows are copied to shared memory with cp.async while the
 // current item's FFTs run (bin 1 only; rows of 4-byte aligned, 4-byte multiple length).
 // SMF: the CTA's dark / gain rows sit in shared memory (every CTA works on one row pair).
@@ -612,27 +617,28 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
         if (live) {
             const long long o1 = (long long)fv.slot * A.slot_stride + (long long)r1 * A.pitch;
             const bool two = r1 + 1 < R;
+            // one store loop per ring type (no per-column type dispatch). Columns c = j + G q:
+            // q < 16 covers c < N/2, which holds the row's C columns (the entry points
+            // require N >= 2 C) and, for the rings the host builds, the whole pitch; the
+            // columns of a wider pitch (up to N) are padding and get zeros in the second loop
+            auto put = [&](auto* ring) {
+                auto* o = ring + o1;
 #pragma unroll
-            for (int q = 0; q < 32; ++q) {
-                const int c = j + G * q;
-                if (c < A.pitch) {
-                    const float y1 = c < C ? x[q].x : 0.f;
-                    const float y2 = c < C ? -x[q].y : 0.f;
-                    if (A.dtype == MR_F32) {
-                        float* o = static_cast<float*>(A.ring) + o1 + c;
-                        o[0] = y1;
-                        if (two) o[A.pitch] = y2;
-                    } else if (A.dtype == MR_BF16) {
-                        __nv_bfloat16* o = static_cast<__nv_bfloat16*>(A.ring) + o1 + c;
-                        o[0] = __float2bfloat16_rn(y1);
-                        if (two) o[A.pitch] = __float2bfloat16_rn(y2);
-                    } else {
-                        __half* o = static_cast<__half*>(A.ring) + o1 + c;
-                        o[0] = __float2half_rn(y1);
-                        if (two) o[A.pitch] = __float2half_rn(y2);
+                for (int q = 0; q < 16; ++q) {
+                    const int c = j + G * q;
+                    if (c < A.pitch) {
+                        o[c] = ring_cvt(o, c < C ? x[q].x : 0.f);
+                        if (two) o[c + A.pitch] = ring_cvt(o, c < C ? -x[q].y : 0.f);
                     }
                 }
-            }
+                for (int c = N / 2 + j; c < min(A.pitch, N); c += G) {
+                    o[c] = ring_cvt(o, 0.f);
+                    if (two) o[c + A.pitch] = ring_cvt(o, 0.f);
+                }
+            };
+            if (A.dtype == MR_F32) put(static_cast<float*>(A.ring));
+            else if (A.dtype == MR_BF16) put(static_cast<__nv_bfloat16*>(A.ring));
+            else put(static_cast<__half*>(A.ring));
         }
     }
 }
