@@ -600,8 +600,11 @@ __global__ void __launch_bounds__(256, 2) fft_filter_kernel(Filter2Args A, int s
 #pragma unroll
         for (int q = 16; q < 32; ++q) x[q] = make_float2(0.f, 0.f);
         const float g = fv.gain * fv.out_scale;
-        // forward FFT, conj(H X), forward FFT again (= N * conj of the inverse): one call site
-#pragma unroll 1
+        // forward FFT, conj(H X), forward FFT again (= N * conj of the inverse): one call site,
+        // except at 1024 points, where two copies let the output permutation of the first
+        // transform stay a renaming of registers
+        constexpr int IT_UNROLL = LOG2N == 10 ? 2 : 1;
+#pragma unroll (IT_UNROLL)
         for (int it = 0; it < 2; ++it) {
             fft::fft_any<LOG2N, SPLIT>(x, buf, T, A.tw, j);
             if (it == 0) {
