@@ -105,11 +105,12 @@ def test_raw_ingest_matches_flexray_correction_plus_fdk(cuda, bin_, flip):
     assert rel_l2(got, want) < 2e-6
 
 
-@pytest.mark.parametrize("cols,flip", [(700, False), (1944, True)])
+@pytest.mark.parametrize("cols,flip", [(700, False), (1944, True), (2040, False)])
 def test_raw_ingest_wide_rows(cuda, cols, flip):
     """2048- and 4096-point rows: the ingest keeps each CTA on one row pair with the pair's
-    dark / gain rows in shared memory next to float exchange buffers. Odd row count (the last
-    pair has one row), more views than one CTA's slots, per-pixel fields."""
+    dark / gain rows in shared memory next to float exchange buffers; at 2040 columns those
+    no longer fit beside two CTAs an SM and the CTAs stride over all items. Odd row count
+    (the last pair has one row), more views than one CTA's slots, per-pixel fields."""
     from oracle import geometry as og
     rng = np.random.default_rng(cols)
     rows, k = 5, 37
