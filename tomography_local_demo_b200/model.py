@@ -217,7 +217,7 @@ def extract_surface(vol, origin, spacing, iso, smooth=15, min_piece=0.002, decim
     lambda|mu iterations (the reference calls VTK's windowed-sinc variant). Decimation is
     not provided here (decimate must be 0)."""
     if decimate and float(decimate) > 0:
-        raise ValueError("decimation is not provided by this build: use decimate=0")
+        raise ValueError("decimation is not provided by this library: use decimate=0")
     points, faces = marching_cubes(vol, iso, origin, spacing)
     if len(faces) == 0:
         raise ValueError(f"no surface at iso={iso:g}; try a lower --iso")
